@@ -1,0 +1,368 @@
+"""MFS solves/s on one B200: mixed precision + batched vs the plain FP64 path.
+
+Workload (default "ellipsoids32"): 32 ellipsoids x 2000 area-sampled points
+(N = Nf = 64000, seeded), 192 rigid-mode right-hand sides, rho 3,
+lambda 1.5, relative residual 1e-8 FP64-verified.  One step = one scene
+solve: supernodal KL factor + PCG for all 192 columns, inputs resident in
+HBM.  The host ordering / pattern of the step is reported separately.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  Under torchrun every rank solves its own
+scene (replicas, weak scaling) and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MFS solves/s at rel-res 1e-8 on 1 B200: mixed+batched+learned vs plain FP64"
+
+WORKLOADS = {
+    # name: (builder, description)
+    "ellipsoids32": (lambda seed: _ell(32, 2000, seed), "32 ellipsoids x 2000 points, N=Nf=64000, R=192"),
+    "ellipsoids8": (lambda seed: _ell(8, 2000, seed), "8 ellipsoids x 2000 points, N=Nf=16000, R=48"),
+    "coins16": (lambda seed: _coins(seed), "16 coins x 4000 points, N=Nf=64000, R=96"),
+    "sphere": (lambda seed: _sphere(), "unit icosphere subdivision 4, N=Nf=2562, R=6"),
+}
+
+
+def _ell(nb, pts, seed):
+    from fastmbcui_b200 import scenes as S
+
+    return S.ellipsoids_scene(nb, pts, seed=seed)
+
+
+def _coins(seed):
+    from fastmbcui_b200 import scenes as S
+
+    return S.coins_scene(pose_seed=seed)
+
+
+def _sphere():
+    from fastmbcui_b200 import scenes as S
+
+    return S.sphere_scene()
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for k, nm in enumerate(names):
+                    if "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                        reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        return dist, int(os.environ["RANK"]), ws, int(os.environ.get("LOCAL_RANK", "0"))
+    return None, 0, 1, 0
+
+
+def _max_over_ranks(dist, v: float) -> float:
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_ours(args):
+    import torch
+
+    import fastmbcui_b200 as F
+
+    dist, rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    build, desc = WORKLOADS[args.workload]
+    sc = build(4 + rank)  # one scene per rank (replicas)
+    Fm = sc.rhs()
+    R = Fm.shape[1]
+    t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
+
+    # host plan (ordering, pattern, supernodes): reported as its own column
+    t0 = time.perf_counter()
+    plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
+    t_plan = time.perf_counter() - t0
+    x, nx, y, Fd = t(sc.x), t(sc.nx), t(sc.y), t(Fm)
+    solver = F.Solver(plan, x=x, nx=nx, y=y, coef=sc.coef, precision=F.MBC_F32)
+    opts = dict(tol=1e-8, max_iters=args.max_iters, max_refine=6, inner_tol=1e-4, check_every=8)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+
+    def step(profile=0):
+        solver.factor()
+        return solver.solve(Fd, out_dtype=torch.float32, profile=profile, **opts)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times, stats = [], []
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            ev0.record()
+            X, st = step(profile=1)
+            ev1.record()
+            torch.cuda.synchronize()
+            times.append(ev0.elapsed_time(ev1))
+            stats.append(st)
+    ms_step = _max_over_ranks(dist, float(np.mean(times)))
+    value = world * 1000.0 / ms_step
+
+    # end to end through the public API: host buffers in, host result out
+    xh, nxh, yh = (np.ascontiguousarray(a, np.float32) for a in (sc.x, sc.nx, sc.y))
+    pin = lambda a: torch.from_numpy(a).pin_memory()
+    hx, hnx, hy, hF = pin(xh), pin(nxh), pin(yh), pin(np.ascontiguousarray(Fm, np.float32))
+    hX = torch.empty((sc.n, R), dtype=torch.float32).pin_memory()
+    e2e_ms = []
+    for k in range(max(1, args.e2e_steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dx, dnx, dy, dF = (a.to(dev, non_blocking=True) for a in (hx, hnx, hy, hF))
+        pl2 = F.Plan(yh.astype(np.float64), sc.rho, sc.lam, sc.max_super)
+        s2 = F.Solver(pl2, x=dx, nx=dnx, y=dy, coef=sc.coef, precision=F.MBC_F32).factor()
+        X2, _ = s2.solve(dF, out_dtype=torch.float32, **opts)
+        hX.copy_(X2)
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - t0) * 1000)
+        del s2, pl2
+    e2e = world * 1000.0 / _max_over_ranks(dist, float(np.mean(e2e_ms)))
+    h2d = (xh.nbytes + nxh.nbytes + yh.nbytes + Fm.size * 4)
+    d2h = sc.n * R * 4
+
+    # plain FP64 GPU path: one cold-started PCG per column; bounded sample of
+    # columns, extrapolated to all R (each column is an independent solve)
+    plain = F.Solver(plan, x=x, nx=nx, y=y, coef=sc.coef, precision=F.MBC_F64)
+    ncol = min(R, args.plain_cols)
+    cols = np.linspace(0, R - 1, ncol).astype(int)
+    torch.cuda.synchronize()
+    ev0.record()
+    plain.factor()
+    ev1.record()
+    torch.cuda.synchronize()
+    t_fac64 = ev0.elapsed_time(ev1)
+    ev0.record()
+    Xp, stp = plain.solve(t(Fm[:, cols], torch.float64), tol=1e-8, max_iters=args.max_iters,
+                          schedule=F.MBC_SCHED_PER_RHS, check_every=8)
+    ev1.record()
+    torch.cuda.synchronize()
+    t_cols = ev0.elapsed_time(ev1)
+    plain_ms = t_fac64 + t_cols * R / ncol
+    plain_sps = 1000.0 / _max_over_ranks(dist, plain_ms)
+
+    # roofline of the dominant kernel (the K / K^T matvec), live CUDA events
+    st = stats[-1]
+    hbm, bf16, src = _peaks()
+    launch_ms = st["t_matvec_ms"] / max(1, st["n_matvec"])
+    flops = float(sc.nf) * sc.n * (20 + 2 * R)
+    achieved = flops / (launch_ms * 1e-3) / 1e12
+    roofline = {"bound": "tensor", "achieved": round(achieved, 2), "peak": bf16, "unit": "TFLOP/s",
+                "frac": round(achieved / bf16, 4), "traffic": None,
+                "kernel": "pk_rows_kernel / pk_cols_kernel (FP32 SIMT, 64-column chunks)",
+                "launch_ms": round(launch_ms, 3), "peak_source": f"bf16 dense, {src}",
+                "fp32_simt_nominal_tflops": 74.4}
+    out = {
+        "metric": METRIC, "value": round(value, 5), "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded scene)",
+        "config": {"workload": args.workload, "desc": desc, "N": sc.n, "Nf": sc.nf, "R": R,
+                   "rho": sc.rho, "lambda": sc.lam, "tol": 1e-8, "precision": "mixed FP32/FP64 refine",
+                   "schedule": "batched", "learned_warm_start": False,
+                   "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas{world}"},
+        "e2e": {"value": round(e2e, 5), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "includes": "H2D, host plan, factor, solve, D2H"},
+        "gpu_launches": int(st["kernel_launches"]) + 4 * 10,
+        "plain_fp64": {"solves_per_s": round(plain_sps, 6), "ms_per_solve": round(plain_ms, 1),
+                       "sample": f"{ncol} of {R} columns, per-RHS cold start, extrapolated",
+                       "iters_max": int(stp["iters_max"])},
+        "speedup_vs_plain_fp64": round(value / plain_sps, 2),
+        "solve": {"iters_max": int(st["iters_max"]), "refinements": int(st["refinements"]),
+                  "true_relres_max": st["true_relres_max"], "n_converged": int(st["n_converged"])},
+        "host_plan_ms": round(t_plan * 1000, 1),
+        "roofline": roofline,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(sc, st, plan)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    del solver, plain
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(sc, st, plan_gpu=None):
+    """The CPU oracle (FP64 C, OpenMP) on a bounded sample of the same solve."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    O.build()
+    t0 = time.perf_counter()
+    pl = O.plan(sc.y, sc.rho, sc.lam, sc.max_super)
+    t_plan = time.perf_counter() - t0
+    op = O.Op.from_scene(sc)
+    # factor: every 50th supernode, scaled by its share of sum n_s^2
+    sizes = np.diff(pl["set_ptr"]).astype(np.float64)
+    sel = np.arange(0, pl["n_super"], 50)
+    sub = dict(pl)
+    sub["n_super"] = len(sel)
+    sub_sp = np.zeros(len(sel) + 1, np.int32)
+    sub_set = []
+    sub_ptr = np.zeros(len(sel) + 1, np.int32)
+    sub_ind = []
+    for k, s in enumerate(sel):
+        sub_set.append(pl["set_ind"][pl["set_ptr"][s]:pl["set_ptr"][s + 1]])
+        sub_sp[k + 1] = sub_sp[k] + len(sub_set[-1])
+        sub_ind.append(pl["sup_ind"][pl["sup_ptr"][s]:pl["sup_ptr"][s + 1]])
+        sub_ptr[k + 1] = sub_ptr[k] + len(sub_ind[-1])
+    sub["set_ptr"], sub["set_ind"] = sub_sp, np.concatenate(sub_set).astype(np.int32)
+    sub["sup_ptr"], sub["sup_ind"] = sub_ptr, np.concatenate(sub_ind).astype(np.int32)
+    ss = np.diff(sub_sp).astype(np.int64)
+    sub["th_ptr"] = np.concatenate([[0], np.cumsum(ss * ss)]).astype(np.int64)
+    t0 = time.perf_counter()
+    O.factor(op, sub)
+    t_fac = (time.perf_counter() - t0) * (sizes ** 2).sum() / float((ss.astype(np.float64) ** 2).sum())
+    # one PCG iteration for one column: K p and K^T w
+    v = np.random.default_rng(0).standard_normal(sc.n)
+    t0 = time.perf_counter()
+    w = op.K(v)
+    op.KT(w)
+    t_iter = time.perf_counter() - t0
+    R = 6 * sc.n_bodies
+    iters = max(1, int(st["iters_total"] / max(1, R)))
+    total = t_plan + t_fac + iters * R * t_iter
+    return {"value": 1.0 / total, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+            "sample": (f"oracle plan in full ({t_plan:.2f}s), factor of every 50th supernode scaled by "
+                       f"sum n_s^2 ({t_fac:.1f}s), one K+K^T pass for one column ({t_iter:.2f}s) x "
+                       f"{iters} iterations x {R} columns")}
+
+
+def run_reference(args):
+    """The reference's CPU path on the host cores (the oracle port: the
+    reference's own host code cannot be built here beyond the ordering)."""
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    build, desc = WORKLOADS[args.workload]
+    sc = build(4)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    O.build()
+    st = {"iters_total": args.ref_iters * 6 * sc.n_bodies}
+    vals = []
+    for _ in range(max(1, args.warmup)):
+        cpu_baseline(sc, st)
+    samples = []
+    for _ in range(args.steps):
+        b = cpu_baseline(sc, st)
+        vals.append(b["value"])
+        samples.append(b["sample"])
+    v = float(np.mean(vals))
+    out = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene)",
+           "config": {"workload": args.workload, "desc": desc, "N": sc.n, "Nf": sc.nf,
+                      "R": 6 * sc.n_bodies, "iterations_assumed": args.ref_iters},
+           "impl": "reference",
+           "cpu_baseline": {"value": v, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+                            "sample": samples[-1]},
+           "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ellipsoids32", choices=sorted(WORKLOADS))
+    ap.add_argument("--max-iters", type=int, default=3000)
+    ap.add_argument("--plain-cols", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--ref-iters", type=int, default=200)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,209 @@
+"""B200-native MFS solve path (maximin ordering -> KL-Cholesky -> PCG).
+
+Python face of libmbc.so (include/mbc.h).  ``Plan`` is host work and runs
+without a GPU; ``Solver`` needs a CUDA device.  ``fastmbcui_b200.mfs_torch``
+registers the reference's ``mfs_torch`` operators on top of this.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import (MBC_F32, MBC_F64, MBC_OP_DENSE, MBC_OP_POINT_KERNEL, MBC_SCHED_BATCHED,
+                   MBC_SCHED_PER_RHS, MbcError, check, ptr)
+
+__all__ = ["Plan", "Solver", "MbcError", "load", "MBC_F32", "MBC_F64", "MBC_SCHED_BATCHED",
+           "MBC_SCHED_PER_RHS"]
+
+
+def load():
+    return _lib.load()
+
+
+class Plan:
+    """Ordering, pattern and supernodes of a point set (host C++)."""
+
+    def __init__(self, pts, rho: float = 3.0, lam: float = 1.5, max_super: int = 2048,
+                 n_threads: int = 0):
+        L = load()
+        p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        o = _lib.PlanOptions()
+        L.mbc_plan_default_options(C.byref(o))
+        o.rho, o.lambda_, o.max_super, o.n_threads = float(rho), float(lam), int(max_super), int(n_threads)
+        h = C.c_void_p()
+        check(L.mbc_plan_create(p.shape[0], p.ctypes.data, C.byref(o), C.byref(h)), "mbc_plan_create")
+        self._h = h
+        self.n = p.shape[0]
+        self.info = _lib.PlanInfo()
+        L.mbc_plan_get_info(h, C.byref(self.info))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib._lib is not None:
+            _lib._lib.mbc_plan_destroy(h)
+            self._h = None
+
+    def order(self):
+        P = np.empty(self.n, np.int32)
+        s = np.empty(self.n, np.float64)
+        check(load().mbc_plan_get_order(self._h, P.ctypes.data, s.ctypes.data), "get_order")
+        return P, s
+
+    def pattern(self):
+        ptr_ = np.empty(self.n + 1, np.int32)
+        ind = np.empty(max(1, self.info.pattern_nnz), np.int32)
+        check(load().mbc_plan_get_pattern(self._h, ptr_.ctypes.data, ind.ctypes.data), "get_pattern")
+        return ptr_, ind[:self.info.pattern_nnz]
+
+    def supernodes(self):
+        sp = np.empty(self.info.n_super + 1, np.int32)
+        si = np.empty(self.n, np.int32)
+        par = np.empty(self.n, np.int32)
+        check(load().mbc_plan_get_supernodes(self._h, sp.ctypes.data, si.ctypes.data, par.ctypes.data),
+              "get_supernodes")
+        return sp, si, par
+
+    def factor_pattern(self):
+        lp = np.empty(self.n + 1, np.int32)
+        li = np.empty(max(1, self.info.factor_nnz), np.int32)
+        check(load().mbc_plan_get_factor_pattern(self._h, lp.ctypes.data, li.ctypes.data),
+              "get_factor_pattern")
+        return lp, li[:self.info.factor_nnz]
+
+
+def solve_options(**kw) -> _lib.SolveOptions:
+    o = _lib.SolveOptions()
+    load().mbc_solve_default_options(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise TypeError(f"unknown solve option {k}")
+        setattr(o, k, v)
+    return o
+
+
+class Solver:
+    """Device factor + PCG for one plan and one operator (torch CUDA tensors).
+
+    Keep the tensors that define the operator alive as long as the solver.
+    """
+
+    def __init__(self, plan: Plan, *, M=None, x=None, nx=None, y=None, coef: float = 1.0,
+                 precision: int = MBC_F64, stream=None):
+        import torch
+
+        L = load()
+        op = _lib.Operator()
+        if M is not None:
+            assert M.is_cuda and M.dtype == torch.float32 and M.dim() == 2
+            M = M.contiguous()
+            op.kind, op.nf, op.n, op.M, op.ldm = MBC_OP_DENSE, M.shape[0], M.shape[1], M.data_ptr(), M.shape[1]
+            self._keep = (M,)
+        else:
+            xs = [t.contiguous().float() for t in (x, nx, y)]
+            op.kind, op.nf, op.n = MBC_OP_POINT_KERNEL, xs[0].shape[0], xs[2].shape[0]
+            op.x, op.nx, op.y = (t.data_ptr() for t in xs)
+            op.coef = float(coef)
+            self._keep = tuple(xs)
+        self.plan = plan
+        self.precision = precision
+        self.nf, self.n = op.nf, op.n
+        self._stream = stream
+        h = C.c_void_p()
+        check(L.mbc_solver_create(plan.handle, C.byref(op), precision, self._sp(), C.byref(h)),
+              "mbc_solver_create")
+        self._h = h
+
+    def _sp(self):
+        import torch
+
+        s = self._stream if self._stream is not None else torch.cuda.current_stream()
+        return C.c_void_p(s.cuda_stream)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib._lib is not None:
+            _lib._lib.mbc_solver_destroy(h)
+            self._h = None
+
+    def factor(self):
+        check(load().mbc_solver_factor(self._h, self._sp()), "mbc_solver_factor")
+        return self
+
+    def pivot_retries(self) -> int:
+        c = C.c_int32(0)
+        check(load().mbc_solver_get_pivot_retries(self._h, C.byref(c)), "get_pivot_retries")
+        return int(c.value)
+
+    def get_factor(self, theta: bool = False):
+        lval = np.empty(max(1, self.plan.info.factor_nnz), np.float64)
+        th = np.empty(max(1, self.plan.info.theta_nnz), np.float64) if theta else None
+        check(load().mbc_solver_get_factor(self._h, lval.ctypes.data, None if th is None else th.ctypes.data),
+              "get_factor")
+        return (lval[:self.plan.info.factor_nnz], None if th is None else th[:self.plan.info.theta_nnz])
+
+    def _dt(self, t):
+        import torch
+
+        return MBC_F64 if t.dtype == torch.float64 else MBC_F32
+
+    def solve(self, F, X0=None, out_dtype=None, iters=False, ok_not_converged=True, **opts):
+        """Forward solve for every column of F (nf x R); returns (X, stats[, iters])."""
+        import torch
+
+        F = F.contiguous()
+        R = 1 if F.dim() == 1 else F.shape[1]
+        dt = out_dtype or F.dtype
+        X = torch.empty((self.n, R), dtype=dt, device=F.device)
+        if X0 is not None:
+            X0 = X0.to(dt).contiguous()
+        o = solve_options(**opts)
+        st = _lib.SolveStats()
+        it = np.zeros(R, np.int32)
+        s = load().mbc_solve(self._h, R, F.data_ptr(), self._dt(F), X.data_ptr(), self._dt(X),
+                             None if X0 is None else X0.data_ptr(), C.byref(o), C.byref(st),
+                             it.ctypes.data, self._sp())
+        ok = (_lib.MBC_OK, _lib.MBC_NOT_CONVERGED) if ok_not_converged else (_lib.MBC_OK,)
+        check(s, "mbc_solve", ok)
+        X = X[:, 0] if F.dim() == 1 else X
+        return (X, st.as_dict(), it) if iters else (X, st.as_dict())
+
+    def solve_adjoint(self, B, out_dtype=None, iters=False, ok_not_converged=True, **opts):
+        import torch
+
+        B = B.contiguous()
+        R = 1 if B.dim() == 1 else B.shape[1]
+        dt = out_dtype or B.dtype
+        X = torch.empty((self.n, R), dtype=dt, device=B.device)
+        o = solve_options(**opts)
+        st = _lib.SolveStats()
+        it = np.zeros(R, np.int32)
+        s = load().mbc_solve_adjoint(self._h, R, B.data_ptr(), self._dt(B), X.data_ptr(), self._dt(X),
+                                     C.byref(o), C.byref(st), it.ctypes.data, self._sp())
+        ok = (_lib.MBC_OK, _lib.MBC_NOT_CONVERGED) if ok_not_converged else (_lib.MBC_OK,)
+        check(s, "mbc_solve_adjoint", ok)
+        X = X[:, 0] if B.dim() == 1 else X
+        return (X, st.as_dict(), it) if iters else (X, st.as_dict())
+
+    def apply_K(self, V):
+        import torch
+
+        V = V.contiguous()
+        R = 1 if V.dim() == 1 else V.shape[1]
+        W = torch.empty((self.nf, R), dtype=V.dtype, device=V.device)
+        check(load().mbc_apply_K(self._h, R, V.data_ptr(), W.data_ptr(), self._sp()), "mbc_apply_K")
+        return W[:, 0] if V.dim() == 1 else W
+
+    def apply_KT(self, W):
+        import torch
+
+        W = W.contiguous()
+        R = 1 if W.dim() == 1 else W.shape[1]
+        T = torch.empty((self.n, R), dtype=W.dtype, device=W.device)
+        check(load().mbc_apply_KT(self._h, R, W.data_ptr(), T.data_ptr(), self._sp()), "mbc_apply_KT")
+        return T[:, 0] if W.dim() == 1 else T

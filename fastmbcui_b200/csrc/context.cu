@@ -1,0 +1,176 @@
+// The mfs_torch operator bodies on top of the plan and solver:
+//   mbc_minvf_float    <- MinvF_float     (mfs_torch/csrc/mfs_torch_ops.cu:21-197)
+//   mbc_vpl_fast_float <- VpL_fast_float  (mfs_torch/csrc/mfs_torch_ops.cu:199-370)
+// Differences from the reference, all at the boundary:
+//   - no dense copy of M: the column permutation is folded into the matvec;
+//   - all R right-hand sides advance together in one batched PCG (same
+//     per-column recurrences and stopping rule as the reference's serial loop);
+//   - PCG scalars and dot products are FP64 (vectors and matvec FP32);
+//   - the factor cache is this context, not process-wide statics; the adjoint
+//     reuses it only for the same points, M and rho, and refactors otherwise.
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "mbc_internal.h"
+
+using mbc::fail;
+
+struct mbc_context {
+  std::unique_ptr<mbc_plan, mbc_status (*)(mbc_plan *)> plan{nullptr, mbc_plan_destroy};
+  std::unique_ptr<mbc_solver, mbc_status (*)(mbc_solver *)> solver{nullptr, mbc_solver_destroy};
+  std::vector<float> key_pts;
+  const float *key_M = nullptr;
+  int32_t key_nf = 0;
+  double key_rho = 0;
+  bool has_forward = false;
+  mbc_solve_stats last{};
+};
+
+extern "C" mbc_status mbc_context_create(mbc_context **out)
+{
+  if (!out) return fail(MBC_BAD_ARG, "out is NULL");
+  *out = new (std::nothrow) mbc_context();
+  return *out ? MBC_OK : fail(MBC_NO_MEMORY, "context allocation failed");
+}
+
+extern "C" mbc_status mbc_context_destroy(mbc_context *ctx)
+{
+  delete ctx;
+  return MBC_OK;
+}
+
+extern "C" mbc_status mbc_context_last_stats(const mbc_context *ctx, mbc_solve_stats *s)
+{
+  if (!ctx || !s) return fail(MBC_BAD_ARG, "NULL argument");
+  *s = ctx->last;
+  return MBC_OK;
+}
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+double ms(clk::time_point a) { return std::chrono::duration<double, std::milli>(clk::now() - a).count(); }
+
+mbc_status check_common(const float *M, int32_t nf, int32_t n, const void *rhs, int32_t R,
+                        const float *Vs_host, float *out)
+{
+  if (!M || !rhs || !Vs_host || !out) return fail(MBC_BAD_ARG, "NULL tensor pointer");
+  if (nf <= 0 || n <= 0 || R <= 0) return fail(MBC_BAD_ARG, "empty operand");
+  return MBC_OK;
+}
+
+// Build (or reuse) the plan + FP32 solver for M and the source points.
+mbc_status prepare(mbc_context *ctx, const float *M, int32_t nf, int32_t n, const float *Vs_host,
+                   double rho, bool allow_reuse, bool timing, cudaStream_t st, bool *reused)
+{
+  *reused = false;
+  const bool same = ctx->solver && ctx->key_M == M && ctx->key_nf == nf && ctx->key_rho == rho &&
+                    (int32_t)ctx->key_pts.size() == 3 * n &&
+                    std::memcmp(ctx->key_pts.data(), Vs_host, sizeof(float) * 3 * (size_t)n) == 0;
+  if (allow_reuse && same) {
+    *reused = true;
+    return MBC_OK;
+  }
+  auto t0 = clk::now();
+  std::vector<double> pts(3 * (size_t)n);
+  for (size_t k = 0; k < pts.size(); ++k) pts[k] = (double)Vs_host[k];  // mfs_torch_ops.cu:46
+  mbc_plan_options po;
+  mbc_plan_default_options(&po);
+  po.rho = rho;  // widened from float inside (mfs_torch_ops.cu:114)
+  mbc_plan *pl = nullptr;
+  mbc_status s = mbc_plan_create(n, pts.data(), &po, &pl);
+  if (s != MBC_OK) return s;
+  ctx->solver.reset();
+  ctx->plan.reset(pl);
+  if (timing) {
+    mbc_plan_info info;
+    mbc_plan_get_info(pl, &info);
+    std::printf("TIME(fps_sampler): %.3f ms\nTIME(pattern): %.3f ms\n", info.t_order_ms,
+                info.t_pattern_ms + info.t_super_ms);
+  }
+  mbc_operator op{};
+  op.kind = MBC_OP_DENSE;
+  op.nf = nf;
+  op.n = n;
+  op.M = M;
+  op.ldm = n;
+  mbc_solver *sv = nullptr;
+  auto t1 = clk::now();
+  s = mbc_solver_create(pl, &op, MBC_F32, (mbc_stream)st, &sv);
+  if (s != MBC_OK) return s;
+  ctx->solver.reset(sv);
+  s = mbc_solver_factor(sv, (mbc_stream)st);
+  if (s != MBC_OK) return s;
+  if (timing) std::printf("TIME(setup+compute): %.3f ms\n", ms(t1));
+  ctx->key_pts.assign(Vs_host, Vs_host + 3 * (size_t)n);
+  ctx->key_M = M;
+  ctx->key_nf = nf;
+  ctx->key_rho = rho;
+  (void)t0;
+  return MBC_OK;
+}
+
+mbc_status run(mbc_context *ctx, bool adjoint, const float *M, int32_t nf, int32_t n, const float *rhs,
+               int32_t R, const float *Vs_host, double rho, int64_t maxit, double tol, int32_t timing,
+               int32_t verbose, float *out, cudaStream_t st)
+{
+  if (!ctx) return fail(MBC_BAD_ARG, "NULL context");
+  mbc_status s = check_common(M, nf, n, rhs, R, Vs_host, out);
+  if (s != MBC_OK) return s;
+  if (adjoint && !ctx->has_forward)
+    return fail(MBC_BAD_ARG, "Float cache tensors are not defined. Please run MinvF_float first.");
+  if (maxit < 0 || maxit > (int64_t)1 << 30) return fail(MBC_BAD_ARG, "pcg_max_iter out of range");
+  auto t0 = clk::now();
+  bool reused = false;
+  s = prepare(ctx, M, nf, n, Vs_host, rho, adjoint, timing != 0, st, &reused);
+  if (s != MBC_OK) return s;
+  mbc_solve_options o;
+  mbc_solve_default_options(&o);
+  o.max_iters = (int32_t)maxit;
+  o.tol = tol;
+  o.max_refine = 0;  // one FP32 sweep: the reference's FP32 PCG with FP64 scalars
+  o.check_every = 4;
+  mbc_solve_stats stats{};
+  std::vector<int32_t> iters(R);
+  auto t1 = clk::now();
+  s = adjoint ? mbc_solve_adjoint(ctx->solver.get(), R, rhs, MBC_F32, out, MBC_F32, &o, &stats,
+                                  iters.data(), (mbc_stream)st)
+              : mbc_solve(ctx->solver.get(), R, rhs, MBC_F32, out, MBC_F32, nullptr, &o, &stats,
+                          iters.data(), (mbc_stream)st);
+  ctx->last = stats;
+  if (s == MBC_NOT_CONVERGED) s = MBC_OK;  // the reference returns after pcg_max_iter silently
+  if (timing) {
+    std::printf("TIME(pcg): %.3f ms\nTIME(total): %.3f ms\n", ms(t1), ms(t0));
+  }
+  if (verbose) {
+    for (int32_t c = 0; c < R; ++c) std::printf("column %d: %d iterations\n", c, iters[c]);
+    std::printf("max relative residual %.3e\n", stats.relres_max);
+  }
+  if (!adjoint && s == MBC_OK) ctx->has_forward = true;
+  return s;
+}
+
+}  // namespace
+
+extern "C" mbc_status mbc_minvf_float(mbc_context *ctx, const float *M, int32_t nf, int32_t n,
+                                      const float *F, int32_t R, const float *Vs_host, double rho,
+                                      int64_t pcg_max_iter, double tol_r, int32_t timing_verbose,
+                                      int32_t solve_verbose, float *out, mbc_stream stream)
+{
+  return run(ctx, false, M, nf, n, F, R, Vs_host, rho, pcg_max_iter, tol_r, timing_verbose,
+             solve_verbose, out, (cudaStream_t)stream);
+}
+
+extern "C" mbc_status mbc_vpl_fast_float(mbc_context *ctx, const float *M, int32_t nf, int32_t n,
+                                         const float *pL, int32_t R, const float *Vs_host, double rho,
+                                         int64_t pcg_max_iter, double tol_r, int32_t timing_verbose,
+                                         int32_t solve_verbose, float *out, mbc_stream stream)
+{
+  return run(ctx, true, M, nf, n, pL, R, Vs_host, rho, pcg_max_iter, tol_r, timing_verbose,
+             solve_verbose, out, (cudaStream_t)stream);
+}

@@ -1,0 +1,1094 @@
+// Device solver for the MFS solve path: operator storage, supernodal KL
+// factor and batched PCG, behind the C ABI in include/mbc.h.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "factor.cuh"
+#include "matvec.cuh"
+#include "mbc_internal.h"
+#include "pcg.cuh"
+#include "solver.h"
+
+namespace mbc {
+
+#define MBC_CK(call)                                                                      \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail(MBC_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+#define MBC_CKL()                                                                         \
+  do {                                                                                     \
+    cudaError_t e_ = cudaGetLastError();                                                   \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail(MBC_CUDA_ERROR, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define MBC_TRY(expr)              \
+  do {                             \
+    mbc_status s_ = (expr);        \
+    if (s_ != MBC_OK) return s_;   \
+  } while (0)
+
+static inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
+
+DevMem::~DevMem() { release(); }
+void DevMem::release()
+{
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+mbc_status DevMem::reserve(size_t b)
+{
+  if (b <= bytes && ptr) return MBC_OK;
+  release();
+  if (b == 0) b = 16;
+  cudaError_t e = cudaMalloc(&ptr, b);
+  if (e != cudaSuccess) {
+    ptr = nullptr;
+    cudaGetLastError();
+    return fail(MBC_NO_MEMORY, std::string("cudaMalloc(") + std::to_string(b) + "): " + cudaGetErrorString(e));
+  }
+  bytes = b;
+  return MBC_OK;
+}
+
+template <typename V>
+static mbc_status upload(DevMem &m, const std::vector<V> &h, cudaStream_t st)
+{
+  MBC_TRY(m.reserve(std::max<size_t>(h.size() * sizeof(V), 16)));
+  if (!h.empty()) MBC_CK(cudaMemcpyAsync(m.ptr, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice, st));
+  return MBC_OK;
+}
+
+// --------------------------------------------------------------------------
+// matvec dispatch
+// --------------------------------------------------------------------------
+namespace {
+
+constexpr int TI_ROWS = 128, TJ_ROWS = 128;
+constexpr int TI_COLS = 128, TJ_COLS = 64;
+
+template <typename T>
+int pick_rc(int R)
+{
+  if (R == 1) return 1;
+  if (R <= 4) return 4;
+  if (R <= 8) return 8;
+  if (R <= 16) return 16;
+  if (sizeof(T) == 8) return 32;
+  return R <= 32 ? 32 : 64;
+}
+
+template <typename T, int RC>
+void rows_launch(const Solver &S, int R, const T *v, T *w, const int32_t *done, cudaStream_t st)
+{
+  if (S.op.kind == MBC_OP_POINT_KERNEL) {
+    dim3 grid(cdiv(S.nf, TI_ROWS), cdiv(R, RC));
+    pk_rows_kernel<T, RC, TI_ROWS, TJ_ROWS><<<grid, TI_ROWS, 0, st>>>(
+        S.x4(), S.n4(), S.nf, S.y4(), S.n, v, R, (T)S.op.coef, w, R, R, done);
+  } else {
+    dim3 grid(cdiv(S.nf, 8), cdiv(R, RC));
+    dense_rows_kernel<T, RC><<<grid, 256, 0, st>>>(S.op.M, S.op.ldm, S.nf, S.n, S.dP(), v, R, w,
+                                                    R, R, done);
+  }
+}
+
+template <typename T, int RC>
+int cols_launch(const Solver &S, int R, const T *w, T *t, const T *pdot, double *part,
+                const int32_t *done, cudaStream_t st)
+{
+  dim3 grid(cdiv(S.n, TI_COLS), cdiv(R, RC));
+  if (S.op.kind == MBC_OP_POINT_KERNEL) {
+    pk_cols_kernel<T, RC, TI_COLS, TJ_COLS><<<grid, TI_COLS, 0, st>>>(
+        S.x4(), S.n4(), S.nf, S.y4(), S.n, w, R, (T)S.op.coef, t, R, R, pdot, part, done);
+  } else {
+    dense_cols_kernel<T, RC, TI_COLS, 32><<<grid, TI_COLS, 0, st>>>(
+        S.op.M, S.op.ldm, S.nf, S.n, S.dP(), w, R, t, R, R, pdot, part, done);
+  }
+  return (int)grid.x;
+}
+
+}  // namespace
+
+template <typename T>
+void launch_rows(const Solver &S, int R, const T *v, T *w, const int32_t *done, cudaStream_t st)
+{
+  switch (pick_rc<T>(R)) {
+    case 1: rows_launch<T, 1>(S, R, v, w, done, st); break;
+    case 4: rows_launch<T, 4>(S, R, v, w, done, st); break;
+    case 8: rows_launch<T, 8>(S, R, v, w, done, st); break;
+    case 16: rows_launch<T, 16>(S, R, v, w, done, st); break;
+    case 32: rows_launch<T, 32>(S, R, v, w, done, st); break;
+    default: rows_launch<T, (sizeof(T) == 8 ? 32 : 64)>(S, R, v, w, done, st); break;
+  }
+}
+
+template <typename T>
+int launch_cols(const Solver &S, int R, const T *w, T *t, const T *pdot, double *part,
+                const int32_t *done, cudaStream_t st)
+{
+  switch (pick_rc<T>(R)) {
+    case 1: return cols_launch<T, 1>(S, R, w, t, pdot, part, done, st);
+    case 4: return cols_launch<T, 4>(S, R, w, t, pdot, part, done, st);
+    case 8: return cols_launch<T, 8>(S, R, w, t, pdot, part, done, st);
+    case 16: return cols_launch<T, 16>(S, R, w, t, pdot, part, done, st);
+    case 32: return cols_launch<T, 32>(S, R, w, t, pdot, part, done, st);
+    default: return cols_launch<T, (sizeof(T) == 8 ? 32 : 64)>(S, R, w, t, pdot, part, done, st);
+  }
+}
+
+int cols_blocks(const Solver &S) { return (int)cdiv(S.n, TI_COLS); }
+
+template void launch_rows<float>(const Solver &, int, const float *, float *, const int32_t *, cudaStream_t);
+template void launch_rows<double>(const Solver &, int, const double *, double *, const int32_t *, cudaStream_t);
+template int launch_cols<float>(const Solver &, int, const float *, float *, const float *, double *, const int32_t *, cudaStream_t);
+template int launch_cols<double>(const Solver &, int, const double *, double *, const double *, double *, const int32_t *, cudaStream_t);
+
+// --------------------------------------------------------------------------
+// factor
+// --------------------------------------------------------------------------
+namespace {
+
+struct ClassSpec {
+  int max_ns;  // inclusive upper bound of n_s for this class (0 = unbounded)
+  int nt, tile_rows;
+};
+// n_s <= 32, <= 64, <= 128 in shared memory; larger ones in global memory
+constexpr ClassSpec kClasses[4] = {{32, 128, 64}, {64, 256, 32}, {128, 512, 32}, {0, 512, 8}};
+
+template <typename T>
+size_t factor_smem(int ns_max, int nt, int tr, bool theta_in_smem)
+{
+  auto al = [](size_t b) { return (b + 15) & ~(size_t)15; };
+  size_t b = al((size_t)ns_max * sizeof(float4)) + al((size_t)tr * ns_max * sizeof(T));
+  if (theta_in_smem) b += al((size_t)(nt / 32) * ns_max * sizeof(T)) + (size_t)ns_max * ns_max * sizeof(T);
+  return b;
+}
+
+template <typename T, typename LT, int NT, int EPT>
+mbc_status launch_factor_class(FactorArgs a, T *theta, LT *lval, size_t smem, cudaStream_t st)
+{
+  auto kern = factor_kernel<T, LT, NT, EPT>;
+  MBC_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<a.count, NT, smem, st>>>(a, theta, lval);
+  MBC_CKL();
+  return MBC_OK;
+}
+
+}  // namespace
+
+// Launch the factor kernels over the given per-class supernode lists.
+template <typename T, typename LT>
+static mbc_status run_factor(Solver &S, const std::vector<int32_t> *lists, T *theta, LT *lval,
+                             double shift, int32_t *d_bad_list, int32_t *d_bad_count,
+                             cudaStream_t st)
+{
+  const Plan &p = *S.plan;
+  for (int c = 0; c < 4; ++c) {
+    const auto &lst = lists[c];
+    if (lst.empty()) continue;
+    DevMem &dl = S.class_list[c];
+    MBC_TRY(upload(dl, lst, st));
+    int ns_max = 0;
+    for (int32_t s : lst) ns_max = std::max(ns_max, p.set_ptr[s + 1] - p.set_ptr[s]);
+    FactorArgs a{};
+    a.list = (const int32_t *)dl.ptr;
+    a.count = (int32_t)lst.size();
+    a.sup_ptr = S.d_sup_ptr();
+    a.sup_ind = S.d_sup_ind();
+    a.set_ptr = S.d_set_ptr();
+    a.set_ind = S.d_set_ind();
+    a.lptr = S.d_lptr();
+    a.th_ptr = S.d_th_ptr();
+    a.kind = S.op.kind;
+    a.xr = S.x4();
+    a.nr = S.n4();
+    a.ys = S.y4();
+    a.M = S.op.M;
+    a.ldm = S.op.ldm;
+    a.Pinv = S.d_Pinv();
+    a.nf = S.nf;
+    a.coef = S.op.coef;
+    a.shift = shift;
+    a.bad_list = d_bad_list;
+    a.bad_count = d_bad_count;
+    const ClassSpec cs = kClasses[c];
+    const bool in_smem = cs.max_ns > 0;
+    int tr = cs.tile_rows;
+    if (!in_smem) {
+      tr = (int)std::max<int64_t>(1, std::min<int64_t>(32, (96 * 1024) / ((int64_t)ns_max * sizeof(T))));
+      MBC_TRY(S.fscratch.reserve((size_t)lst.size() * (cs.nt / 32) * ns_max * sizeof(T)));
+      a.gscratch = S.fscratch.ptr;
+      a.gscratch_stride = ns_max;
+    }
+    a.smem_cap = in_smem ? cs.max_ns : 0;
+    a.tile_rows = tr;
+    const size_t smem = factor_smem<T>(ns_max, cs.nt, tr, in_smem);
+    switch (c) {
+      case 0: MBC_TRY((launch_factor_class<T, LT, 128, 5>(a, theta, lval, smem, st))); break;
+      case 1: MBC_TRY((launch_factor_class<T, LT, 256, 9>(a, theta, lval, smem, st))); break;
+      case 2: MBC_TRY((launch_factor_class<T, LT, 512, 17>(a, theta, lval, smem, st))); break;
+      default: MBC_TRY((launch_factor_class<T, LT, 512, 16>(a, theta, lval, smem, st))); break;
+    }
+  }
+  return MBC_OK;
+}
+
+static void split_classes(const Plan &p, const std::vector<int32_t> &ids, std::vector<int32_t> *lists)
+{
+  for (int c = 0; c < 4; ++c) lists[c].clear();
+  for (int32_t s : ids) {
+    const int ns = p.set_ptr[s + 1] - p.set_ptr[s];
+    int c = 3;
+    for (int k = 0; k < 3; ++k)
+      if (ns <= kClasses[k].max_ns) {
+        c = k;
+        break;
+      }
+    lists[c].push_back(s);
+  }
+  // largest first inside a class: the long CTAs start early
+  for (int c = 0; c < 4; ++c)
+    std::stable_sort(lists[c].begin(), lists[c].end(), [&](int32_t a, int32_t b) {
+      return p.set_ptr[a + 1] - p.set_ptr[a] > p.set_ptr[b + 1] - p.set_ptr[b];
+    });
+}
+
+mbc_status Solver::factor(cudaStream_t st)
+{
+  const Plan &p = *plan;
+  const size_t th_n = (size_t)p.th_ptr.back();
+  const size_t l_n = (size_t)p.lptr.back();
+  const size_t esz = precision == MBC_F64 ? 8 : 4;
+  MBC_TRY(theta.reserve(std::max<size_t>(th_n * esz, 16)));
+  MBC_TRY(lval.reserve(std::max<size_t>(l_n * esz, 16)));
+  MBC_TRY(bad.reserve(sizeof(int32_t) * (p.n_super + 1)));
+  MBC_CK(cudaMemsetAsync(bad.ptr, 0, sizeof(int32_t), st));
+  int32_t *d_bad_count = (int32_t *)bad.ptr;
+  int32_t *d_bad_list = d_bad_count + 1;
+  std::vector<int32_t> all(p.n_super);
+  for (int32_t s = 0; s < p.n_super; ++s) all[s] = s;
+  std::vector<int32_t> lists[4];
+  split_classes(p, all, lists);
+  if (precision == MBC_F64)
+    MBC_TRY((run_factor<double, double>(*this, lists, (double *)theta.ptr, (double *)lval.ptr, 0.0,
+                                        d_bad_list, d_bad_count, st)));
+  else
+    MBC_TRY((run_factor<float, float>(*this, lists, (float *)theta.ptr, (float *)lval.ptr, 0.0,
+                                      d_bad_list, d_bad_count, st)));
+  // supernodes with a non-positive pivot: redo in FP64, then FP64 with a
+  // small diagonal shift
+  pivot_retries = 0;
+  const double shifts[2] = {0.0, 1e-10};
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    int32_t nbad = 0;
+    MBC_CK(cudaMemcpyAsync(&nbad, d_bad_count, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    MBC_CK(cudaStreamSynchronize(st));
+    if (nbad == 0) break;
+    if (precision == MBC_F64 && attempt == 0) continue;  // FP64 already: go to the shift
+    std::vector<int32_t> ids(nbad);
+    MBC_CK(cudaMemcpy(ids.data(), d_bad_list, sizeof(int32_t) * nbad, cudaMemcpyDeviceToHost));
+    pivot_retries += nbad;
+    MBC_CK(cudaMemsetAsync(d_bad_count, 0, sizeof(int32_t), st));
+    split_classes(p, ids, lists);
+    MBC_TRY(theta64.reserve(std::max<size_t>(th_n * 8, 16)));
+    if (precision == MBC_F64)
+      MBC_TRY((run_factor<double, double>(*this, lists, (double *)theta.ptr, (double *)lval.ptr,
+                                          shifts[attempt], d_bad_list, d_bad_count, st)));
+    else
+      MBC_TRY((run_factor<double, float>(*this, lists, (double *)theta64.ptr, (float *)lval.ptr,
+                                         shifts[attempt], d_bad_list, d_bad_count, st)));
+  }
+  {
+    int32_t nbad = 0;
+    MBC_CK(cudaMemcpyAsync(&nbad, d_bad_count, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    MBC_CK(cudaStreamSynchronize(st));
+    if (nbad > 0) {
+      // the shifted FP64 retry also failed: count it but keep its columns
+      // from the retry (precision F64 shifts directly); report the status
+      factored = false;
+      return fail(MBC_NONSPD_PIVOT, std::to_string(nbad) + " supernode(s) not positive definite");
+    }
+  }
+  factored = true;
+  return MBC_OK;
+}
+
+// --------------------------------------------------------------------------
+// solver creation
+// --------------------------------------------------------------------------
+mbc_status Solver::create(const Plan &pl, const mbc_operator &o, int32_t prec, cudaStream_t st)
+{
+  plan = &pl;
+  op = o;
+  precision = prec;
+  n = pl.n;
+  nf = o.nf;
+  MBC_TRY(upload(m_P, pl.P, st));
+  MBC_TRY(upload(m_Pinv, pl.Pinv, st));
+  MBC_TRY(upload(m_sup_ptr, pl.sup_ptr, st));
+  MBC_TRY(upload(m_sup_ind, pl.sup_ind, st));
+  MBC_TRY(upload(m_set_ptr, pl.set_ptr, st));
+  MBC_TRY(upload(m_set_ind, pl.set_ind, st));
+  MBC_TRY(upload(m_lptr, pl.lptr, st));
+  MBC_TRY(upload(m_lind, pl.lind, st));
+  MBC_TRY(upload(m_rptr, pl.rptr, st));
+  MBC_TRY(upload(m_rcol, pl.rcol, st));
+  MBC_TRY(upload(m_rmap, pl.rmap, st));
+  MBC_TRY(upload(m_th_ptr, pl.th_ptr, st));
+  if (o.kind == MBC_OP_POINT_KERNEL) {
+    MBC_TRY(m_x4.reserve(sizeof(float4) * nf));
+    MBC_TRY(m_n4.reserve(sizeof(float4) * nf));
+    MBC_TRY(m_y4.reserve(sizeof(float4) * n));
+    pack_points_kernel<<<cdiv(nf, 256), 256, 0, st>>>(nf, o.x, nullptr, (float4 *)m_x4.ptr);
+    pack_points_kernel<<<cdiv(nf, 256), 256, 0, st>>>(nf, o.nx, nullptr, (float4 *)m_n4.ptr);
+    pack_points_kernel<<<cdiv(n, 256), 256, 0, st>>>(n, o.y, (const int32_t *)m_Pinv.ptr,
+                                                     (float4 *)m_y4.ptr);
+    MBC_CKL();
+  }
+  MBC_CK(cudaStreamSynchronize(st));
+  return MBC_OK;
+}
+
+// --------------------------------------------------------------------------
+// PCG
+// --------------------------------------------------------------------------
+namespace {
+
+struct Layout2D {
+  dim3 block, grid;
+  size_t smem;
+};
+
+Layout2D layout2d(int n, int R)
+{
+  int bx = 1;
+  while (bx < R && bx < 32) bx <<= 1;
+  const int by = 256 / bx;
+  Layout2D L;
+  L.block = dim3(bx, by);
+  L.grid = dim3(cdiv(n, by), cdiv(R, bx));
+  L.smem = sizeof(double) * 256;
+  return L;
+}
+
+}  // namespace
+
+// Work buffers for one precision.
+template <typename T>
+struct PcgWork {
+  T *X, *Rv, *Pv, *Z, *U, *Tt, *W;
+  double *part;
+  int part_stride;  // blocks
+  PcgScalars sc;
+};
+
+template <typename T>
+static mbc_status pcg_buffers(Solver &S, int R, PcgWork<T> &w)
+{
+  const size_t nv = (size_t)S.n * R, fv = (size_t)S.nf * R;
+  const size_t vb = ((nv * sizeof(T)) + 255) & ~(size_t)255;
+  const size_t fb = ((fv * sizeof(T)) + 255) & ~(size_t)255;
+  DevMem &m = sizeof(T) == 8 ? S.work64 : S.work32;
+  MBC_TRY(m.reserve(6 * vb + fb));
+  char *b = (char *)m.ptr;
+  w.X = (T *)b;
+  w.Rv = (T *)(b + vb);
+  w.Pv = (T *)(b + 2 * vb);
+  w.Z = (T *)(b + 3 * vb);
+  w.U = (T *)(b + 4 * vb);
+  w.Tt = (T *)(b + 5 * vb);
+  w.W = (T *)(b + 6 * vb);
+  const int nblk = std::max<int>(std::max<int>(cols_blocks(S), layout2d(S.n, R).grid.x), 1);
+  w.part_stride = nblk;
+  MBC_TRY(S.part.reserve(sizeof(double) * (size_t)nblk * R));
+  w.part = (double *)S.part.ptr;
+  MBC_TRY(S.scal.reserve(sizeof(double) * 7 * R + sizeof(int32_t) * (2 * R + 4)));
+  double *d = (double *)S.scal.ptr;
+  w.sc.rz = d;
+  w.sc.b2 = d + R;
+  w.sc.thr = d + 2 * R;
+  w.sc.alpha = d + 3 * R;
+  w.sc.beta = d + 4 * R;
+  w.sc.rr = d + 5 * R;
+  w.sc.pt = d + 6 * R;
+  int32_t *ii = (int32_t *)(d + 7 * R);
+  w.sc.status = ii;
+  w.sc.iters = ii + R;
+  w.sc.done = ii + 2 * R;
+  return MBC_OK;
+}
+
+__global__ void set_status_kernel(int R, int32_t *status, int32_t *iters, int32_t *done,
+                                  const int32_t *mask)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c == 0) *done = 0;
+  if (c >= R) return;
+  status[c] = (mask == nullptr || mask[c]) ? COL_ACTIVE : COL_OK;
+  iters[c] = 0;
+}
+
+// Warm starts: thresholds relative to |b|^2 of the original right-hand side.
+__global__ void set_thresholds_kernel(int R, double tol2, const double *b2ref, PcgScalars sc)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= R) return;
+  sc.b2[c] = b2ref[c];
+  sc.thr[c] = tol2 * b2ref[c];
+  if (b2ref[c] < 1e-16 && sc.status[c] == COL_ACTIVE) sc.status[c] = COL_OK;
+}
+
+// Run PCG on (K^T K) x = b for R columns.  On entry w.Rv holds b (new order)
+// and w.X the starting point whose residual b - K^T K x is already in w.Rv.
+// Columns with mask[c] == 0 are skipped.  Returns after every column stopped.
+template <typename T, typename LT>
+static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, const LT *lval, int maxit, double tol,
+                          bool precond, int check_every, const int32_t *d_mask, cudaStream_t st,
+                          const double *d_b2ref = nullptr)
+{
+  const Plan &p = *S.plan;
+  const Layout2D L = layout2d(S.n, R);
+  const int nblk2 = (int)L.grid.x;
+  w.sc.maxit = maxit;
+  w.sc.tol2 = tol * tol;
+  set_status_kernel<<<cdiv(R, 256), 256, 0, st>>>(R, w.sc.status, w.sc.iters, w.sc.done, d_mask);
+  // |b|^2 and the stopping thresholds
+  dot_partial_kernel<T><<<L.grid, L.block, L.smem, st>>>(S.n, R, w.Rv, w.Rv, w.part);
+  reduce_kernel<<<1, 1024, 0, st>>>(nblk2, R, w.part, RED_INIT_B, w.sc, nullptr);
+  if (d_b2ref) set_thresholds_kernel<<<cdiv(R, 256), 256, 0, st>>>(R, w.sc.tol2, d_b2ref, w.sc);
+  // z = L L^T r, rz = r.z, p = z
+  auto apply_precond = [&](const T *r, T *z) {
+    if (precond) {
+      precond_lt_kernel<T, LT><<<L.grid, L.block, 0, st>>>(S.n, R, S.d_lptr(), S.d_lind(), lval, r,
+                                                            w.U, w.sc.done);
+      precond_l_kernel<T, LT><<<L.grid, L.block, L.smem, st>>>(S.n, R, S.d_rptr(), S.d_rcol(),
+                                                               S.d_rmap(), lval, w.U, z, r, w.part,
+                                                               w.sc.done);
+    } else {
+      cudaMemcpyAsync(z, r, sizeof(T) * (size_t)S.n * R, cudaMemcpyDeviceToDevice, st);
+      dot_partial_kernel<T><<<L.grid, L.block, L.smem, st>>>(S.n, R, r, z, w.part);
+    }
+  };
+  apply_precond(w.Rv, w.Pv);
+  reduce_kernel<<<1, 1024, 0, st>>>(nblk2, R, w.part, RED_STORE, w.sc, w.sc.rz);
+  MBC_CKL();
+  (void)p;
+  S.launches += (d_b2ref ? 4 : 3) + 3;
+  int32_t *h_done = S.h_flag;
+  if (S.profile) MBC_TRY(S.ensure_events(2 * check_every));
+  for (int it = 0; it < maxit; it += check_every) {
+    const int kmax = std::min(check_every, maxit - it);
+    for (int k = 0; k < kmax; ++k) {
+      if (S.profile) MBC_CK(cudaEventRecord(S.events[2 * k], st));
+      launch_rows<T>(S, R, w.Pv, w.W, w.sc.done, st);
+      const int nb = launch_cols<T>(S, R, w.W, w.Tt, w.Pv, w.part, w.sc.done, st);
+      if (S.profile) MBC_CK(cudaEventRecord(S.events[2 * k + 1], st));
+      reduce_kernel<<<1, 1024, 0, st>>>(nb, R, w.part, RED_ALPHA, w.sc, nullptr);
+      update_xr_kernel<T><<<L.grid, L.block, L.smem, st>>>(S.n, R, w.sc.alpha, w.Pv, w.Tt, w.X,
+                                                           w.Rv, w.part, w.sc.done);
+      reduce_kernel<<<1, 1024, 0, st>>>(nblk2, R, w.part, RED_CHECK, w.sc, nullptr);
+      apply_precond(w.Rv, w.Z);
+      reduce_kernel<<<1, 1024, 0, st>>>(nblk2, R, w.part, RED_BETA, w.sc, nullptr);
+      update_p_kernel<T><<<L.grid, L.block, 0, st>>>(S.n, R, w.sc.beta, w.sc.status, w.Z, w.Pv,
+                                                      w.sc.done);
+      S.launches += 9;
+    }
+    MBC_CKL();
+    MBC_CK(cudaMemcpyAsync(h_done, w.sc.done, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    MBC_CK(cudaStreamSynchronize(st));
+    if (S.profile) {
+      // only iterations that still had an active column did real work; the
+      // done flag is read at the start of each matvec kernel
+      for (int k = 0; k < kmax; ++k) {
+        float ms = 0.f;
+        MBC_CK(cudaEventElapsedTime(&ms, S.events[2 * k], S.events[2 * k + 1]));
+        S.prof_ms_all.push_back(ms);
+      }
+    }
+    if (*h_done) break;
+  }
+  return MBC_OK;
+}
+
+// residual r = K^T (f - K x) in T, all columns; f, x new-order buffers
+template <typename T>
+static void residual(Solver &S, int R, const T *F, const T *X, T *W, T *Rout, cudaStream_t st)
+{
+  launch_rows<T>(S, R, X, W, nullptr, st);
+  const int64_t cnt = (int64_t)S.nf * R;
+  sub_kernel<T><<<cdiv(cnt, 256), 256, 0, st>>>(cnt, F, W, W);
+  launch_cols<T>(S, R, W, Rout, nullptr, nullptr, nullptr, st);
+  S.launches += 3;
+}
+
+// per-column norms^2 of an n x R array into host vector
+template <typename T>
+static mbc_status col_norms2(Solver &S, int R, const T *A, std::vector<double> &out, cudaStream_t st)
+{
+  const Layout2D L = layout2d(S.n, R);
+  // own buffer: S.part may be referenced by a live PcgWork
+  MBC_TRY(S.nrm.reserve(sizeof(double) * ((size_t)L.grid.x * R + R)));
+  double *part = (double *)S.nrm.ptr;
+  double *res = part + (size_t)L.grid.x * R;
+  dot_partial_kernel<T><<<L.grid, L.block, L.smem, st>>>(S.n, R, A, A, part);
+  PcgScalars sc{};
+  reduce_kernel<<<1, 1024, 0, st>>>((int)L.grid.x, R, part, RED_STORE, sc, res);
+  S.launches += 2;
+  MBC_CKL();
+  out.resize(R);
+  MBC_CK(cudaMemcpyAsync(out.data(), res, sizeof(double) * R, cudaMemcpyDeviceToHost, st));
+  MBC_CK(cudaStreamSynchronize(st));
+  return MBC_OK;
+}
+
+// per-column norms^2 of an n x R array into a device vector (R doubles)
+template <typename T>
+static mbc_status col_norms2_dev(Solver &S, int R, const T *A, double *out, cudaStream_t st)
+{
+  const Layout2D L = layout2d(S.n, R);
+  MBC_TRY(S.nrm.reserve(sizeof(double) * (size_t)L.grid.x * R));
+  double *part = (double *)S.nrm.ptr;
+  dot_partial_kernel<T><<<L.grid, L.block, L.smem, st>>>(S.n, R, A, A, part);
+  PcgScalars sc{};
+  reduce_kernel<<<1, 1024, 0, st>>>((int)L.grid.x, R, part, RED_STORE, sc, out);
+  S.launches += 2;
+  MBC_CKL();
+  return MBC_OK;
+}
+
+template <typename S_, typename D_>
+static void convert(int64_t cnt, const S_ *a, D_ *b, cudaStream_t st)
+{
+  convert_kernel<S_, D_><<<cdiv(cnt, 256), 256, 0, st>>>(cnt, a, b);
+}
+
+template <typename D_>
+static void permute_in(Solver &S, int R, const void *src, int32_t dt, D_ *dst, cudaStream_t st)
+{
+  const int64_t cnt = (int64_t)S.n * R;
+  ++S.launches;
+  if (dt == MBC_F64)
+    permute_in_kernel<double, D_><<<cdiv(cnt, 256), 256, 0, st>>>(S.n, R, S.dP(), (const double *)src, dst);
+  else
+    permute_in_kernel<float, D_><<<cdiv(cnt, 256), 256, 0, st>>>(S.n, R, S.dP(), (const float *)src, dst);
+}
+
+template <typename S_>
+static void permute_out(Solver &S, int R, const S_ *src, void *dst, int32_t dt, cudaStream_t st)
+{
+  const int64_t cnt = (int64_t)S.n * R;
+  ++S.launches;
+  if (dt == MBC_F64)
+    permute_out_kernel<S_, double><<<cdiv(cnt, 256), 256, 0, st>>>(S.n, R, S.dP(), src, (double *)dst);
+  else
+    permute_out_kernel<S_, float><<<cdiv(cnt, 256), 256, 0, st>>>(S.n, R, S.dP(), src, (float *)dst);
+}
+
+template <typename D_>
+static void load_rows(Solver &S, int R, const void *src, int32_t dt, D_ *dst, cudaStream_t st)
+{
+  const int64_t cnt = (int64_t)S.nf * R;
+  ++S.launches;
+  if (dt == MBC_F64) convert<double, D_>(cnt, (const double *)src, dst, st);
+  else convert<float, D_>(cnt, (const float *)src, dst, st);
+}
+
+// Collect per-column results of the last run_pcg into stats.
+template <typename T>
+static mbc_status collect(Solver &S, int R, PcgWork<T> &w, std::vector<int32_t> &status,
+                          std::vector<int32_t> &iters, std::vector<double> &rel, cudaStream_t st)
+{
+  std::vector<double> rr(R), b2(R);
+  status.resize(R);
+  iters.resize(R);
+  MBC_CK(cudaMemcpyAsync(status.data(), w.sc.status, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, st));
+  MBC_CK(cudaMemcpyAsync(iters.data(), w.sc.iters, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, st));
+  MBC_CK(cudaMemcpyAsync(rr.data(), w.sc.rr, sizeof(double) * R, cudaMemcpyDeviceToHost, st));
+  MBC_CK(cudaMemcpyAsync(b2.data(), w.sc.b2, sizeof(double) * R, cudaMemcpyDeviceToHost, st));
+  MBC_CK(cudaStreamSynchronize(st));
+  rel.resize(R);
+  for (int c = 0; c < R; ++c) rel[c] = b2[c] < 1e-16 ? 0.0 : std::sqrt(rr[c] / b2[c]);
+  return MBC_OK;
+}
+
+static mbc_status finish_stats(int R, const std::vector<int32_t> &status, const std::vector<int32_t> &iters,
+                               const std::vector<double> &rel, mbc_solve_stats *st_out,
+                               int32_t *iters_host)
+{
+  mbc_solve_stats s{};
+  s.true_relres_max = -1;
+  int worst = 0;
+  for (int c = 0; c < R; ++c) {
+    s.iters_max = std::max(s.iters_max, iters[c]);
+    s.iters_total += iters[c];
+    if (status[c] == COL_OK) ++s.n_converged;
+    s.relres_max = std::max(s.relres_max, rel[c]);
+    int code = status[c] == COL_OK ? 0 : status[c] == COL_BREAKDOWN ? 2 : 1;
+    worst = std::max(worst, code);
+    if (iters_host) iters_host[c] = iters[c];
+  }
+  s.status_per_worst = worst;
+  if (st_out) *st_out = s;
+  return MBC_OK;
+}
+
+// Plain (MBC_F64) or reference-style single-sweep solve in precision T.
+// mode 0: forward with F; mode 1: adjoint with B.
+template <typename T>
+mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, int32_t x_dt,
+                               const void *X0, bool adjoint, const mbc_solve_options &o,
+                               mbc_solve_stats *stats, int32_t *iters_host, cudaStream_t st)
+{
+  PcgWork<T> w;
+  MBC_TRY(pcg_buffers<T>(*this, R, w));
+  // F (forward) lives in fbuf (T, nf x R)
+  DevMem &fm = sizeof(T) == 8 ? fbuf64 : fbuf32;
+  if (!adjoint) {
+    MBC_TRY(fm.reserve(sizeof(T) * (size_t)nf * R));
+    load_rows<T>(*this, R, rhs, rhs_dt, (T *)fm.ptr, st);
+  }
+  const int64_t nv = (int64_t)n * R;
+  if (X0) {
+    permute_in<T>(*this, R, X0, x_dt, w.X, st);
+    if (adjoint) {
+      // r = b - K^T K x0
+      permute_in<T>(*this, R, rhs, rhs_dt, w.Z, st);
+      launch_rows<T>(*this, R, w.X, w.W, nullptr, st);
+      launch_cols<T>(*this, R, w.W, w.Tt, nullptr, nullptr, nullptr, st);
+      sub_kernel<T><<<cdiv(nv, 256), 256, 0, st>>>(nv, w.Z, w.Tt, w.Rv);
+    } else {
+      residual<T>(*this, R, (const T *)fm.ptr, w.X, w.W, w.Rv, st);
+    }
+  } else {
+    MBC_CK(cudaMemsetAsync(w.X, 0, sizeof(T) * nv, st));
+    if (adjoint) permute_in<T>(*this, R, rhs, rhs_dt, w.Rv, st);
+    else launch_cols<T>(*this, R, (const T *)fm.ptr, w.Rv, nullptr, nullptr, nullptr, st);
+  }
+  MBC_CKL();
+  // A warm start keeps the thresholds relative to |b| (b = K^T f or the adjoint rhs).
+  const double *b2 = nullptr;
+  if (X0) {
+    MBC_TRY(b2ref.reserve(sizeof(double) * R));
+    T *bvec = w.Tt;
+    if (adjoint) permute_in<T>(*this, R, rhs, rhs_dt, bvec, st);
+    else launch_cols<T>(*this, R, (const T *)fm.ptr, bvec, nullptr, nullptr, nullptr, st);
+    MBC_TRY(col_norms2_dev<T>(*this, R, bvec, (double *)b2ref.ptr, st));
+    b2 = (const double *)b2ref.ptr;
+  }
+  if (precision == MBC_F64)
+    MBC_TRY((run_pcg<T, double>(*this, R, w, (const double *)lval.ptr, o.max_iters, o.tol,
+                                o.precondition != 0, std::max(1, o.check_every), nullptr, st, b2)));
+  else
+    MBC_TRY((run_pcg<T, float>(*this, R, w, (const float *)lval.ptr, o.max_iters, o.tol,
+                               o.precondition != 0, std::max(1, o.check_every), nullptr, st, b2)));
+  std::vector<int32_t> status, iters;
+  std::vector<double> rel;
+  MBC_TRY(collect<T>(*this, R, w, status, iters, rel, st));
+  permute_out<T>(*this, R, w.X, X, x_dt, st);
+  MBC_CKL();
+  MBC_TRY(finish_stats(R, status, iters, rel, stats, iters_host));
+  if (stats && o.true_residual && !adjoint) {
+    // FP64 |K^T (f - K x)| / |K^T f| on the result
+    MBC_TRY(true_residual(R, rhs, rhs_dt, X, x_dt, stats, st));
+  }
+  MBC_CK(cudaStreamSynchronize(st));
+  return MBC_OK;
+}
+
+// FP64 true residual of a forward solution (original-order X).
+mbc_status Solver::true_residual(int R, const void *F, int32_t f_dt, const void *X, int32_t x_dt,
+                                 mbc_solve_stats *stats, cudaStream_t st)
+{
+  MBC_TRY(fbuf64.reserve(sizeof(double) * (size_t)nf * R));
+  MBC_TRY(res64.reserve(sizeof(double) * ((size_t)nf * R + 2 * (size_t)n * R)));
+  double *Fd = (double *)fbuf64.ptr;
+  double *Wd = (double *)res64.ptr;
+  double *Xd = Wd + (size_t)nf * R;
+  double *Rd = Xd + (size_t)n * R;
+  load_rows<double>(*this, R, F, f_dt, Fd, st);
+  permute_in<double>(*this, R, X, x_dt, Xd, st);
+  residual<double>(*this, R, Fd, Xd, Wd, Rd, st);
+  launch_cols<double>(*this, R, Fd, Xd, nullptr, nullptr, nullptr, st);  // b = K^T f into Xd
+  MBC_CKL();
+  std::vector<double> nr, nb;
+  MBC_TRY(col_norms2<double>(*this, R, Rd, nr, st));
+  MBC_TRY(col_norms2<double>(*this, R, Xd, nb, st));
+  double m = 0;
+  for (int c = 0; c < R; ++c) m = std::max(m, nb[c] < 1e-16 ? 0.0 : std::sqrt(nr[c] / nb[c]));
+  stats->true_relres_max = m;
+  return MBC_OK;
+}
+
+// Mixed precision: FP32 PCG sweeps inside an FP64 iterative-refinement loop
+// on the true residual r = K^T (f - K x).
+mbc_status Solver::solve_mixed(int R, const void *rhs, int32_t rhs_dt, void *X, int32_t x_dt,
+                               const void *X0, bool adjoint, const mbc_solve_options &o,
+                               mbc_solve_stats *stats, int32_t *iters_host, cudaStream_t st)
+{
+  const size_t nv = (size_t)n * R, fv = (size_t)nf * R;
+  MBC_TRY(fbuf64.reserve(sizeof(double) * fv));
+  MBC_TRY(res64.reserve(sizeof(double) * (fv + 3 * nv)));
+  double *Fd = (double *)fbuf64.ptr;
+  double *Wd = (double *)res64.ptr;
+  double *Xd = Wd + fv;
+  double *Rd = Xd + nv;
+  double *Bd = Rd + nv;
+  if (adjoint) permute_in<double>(*this, R, rhs, rhs_dt, Bd, st);
+  else {
+    load_rows<double>(*this, R, rhs, rhs_dt, Fd, st);
+    launch_cols<double>(*this, R, Fd, Bd, nullptr, nullptr, nullptr, st);
+  }
+  if (X0) permute_in<double>(*this, R, X0, x_dt, Xd, st);
+  else MBC_CK(cudaMemsetAsync(Xd, 0, sizeof(double) * nv, st));
+  MBC_CKL();
+  std::vector<double> nb;
+  MBC_TRY(col_norms2<double>(*this, R, Bd, nb, st));
+  PcgWork<float> w;
+  MBC_TRY(pcg_buffers<float>(*this, R, w));
+  MBC_TRY(mask.reserve(sizeof(int32_t) * R));
+  std::vector<int32_t> hmask(R), it_total(R, 0), status(R, COL_MAXIT);
+  std::vector<double> rel(R, 1.0);
+  int sweeps = 0;
+  const int max_refine = std::max(1, o.max_refine);
+  bool have_x = X0 != nullptr;
+  for (int sweep = 0; sweep <= max_refine; ++sweep) {
+    // true residual
+    if (have_x) {
+      if (adjoint) {
+        launch_rows<double>(*this, R, Xd, Wd, nullptr, st);
+        launch_cols<double>(*this, R, Wd, Rd, nullptr, nullptr, nullptr, st);
+        sub_kernel<double><<<cdiv(nv, 256), 256, 0, st>>>(nv, Bd, Rd, Rd);
+      } else {
+        residual<double>(*this, R, Fd, Xd, Wd, Rd, st);
+      }
+    } else {
+      MBC_CK(cudaMemcpyAsync(Rd, Bd, sizeof(double) * nv, cudaMemcpyDeviceToDevice, st));
+    }
+    std::vector<double> nr;
+    MBC_TRY(col_norms2<double>(*this, R, Rd, nr, st));
+    bool all = true;
+    for (int c = 0; c < R; ++c) {
+      rel[c] = nb[c] < 1e-16 ? 0.0 : std::sqrt(nr[c] / nb[c]);
+      hmask[c] = rel[c] > o.tol;
+      if (hmask[c]) all = false;
+      else status[c] = COL_OK;
+    }
+    if (all || sweep == max_refine) break;
+    // inner FP32 PCG on (K^T K) d = r, relative tolerance inner_tol
+    MBC_CK(cudaMemcpyAsync(mask.ptr, hmask.data(), sizeof(int32_t) * R, cudaMemcpyHostToDevice, st));
+    convert<double, float>((int64_t)nv, Rd, w.Rv, st);
+    MBC_CK(cudaMemsetAsync(w.X, 0, sizeof(float) * nv, st));
+    MBC_TRY((run_pcg<float, float>(*this, R, w, (const float *)lval.ptr, o.max_iters,
+                                   std::max(o.inner_tol, 1e-7), o.precondition != 0,
+                                   std::max(1, o.check_every), (const int32_t *)mask.ptr, st)));
+    std::vector<int32_t> st_in, it_in;
+    std::vector<double> rel_in;
+    MBC_TRY(collect<float>(*this, R, w, st_in, it_in, rel_in, st));
+    for (int c = 0; c < R; ++c) {
+      it_total[c] += it_in[c];
+      if (st_in[c] == COL_BREAKDOWN) status[c] = COL_BREAKDOWN;
+    }
+    accumulate_kernel<float><<<cdiv(nv, 256), 256, 0, st>>>(n, R, w.X, Xd);
+    MBC_CKL();
+    have_x = true;
+    ++sweeps;
+  }
+  permute_out<double>(*this, R, Xd, X, x_dt, st);
+  MBC_CKL();
+  for (int c = 0; c < R; ++c)
+    if (status[c] != COL_OK && status[c] != COL_BREAKDOWN) status[c] = COL_MAXIT;
+  MBC_TRY(finish_stats(R, status, it_total, rel, stats, iters_host));
+  if (stats) {
+    stats->refinements = sweeps;
+    double m = 0;
+    for (int c = 0; c < R; ++c) m = std::max(m, rel[c]);
+    stats->true_relres_max = m;
+    stats->relres_max = m;
+  }
+  MBC_CK(cudaStreamSynchronize(st));
+  return MBC_OK;
+}
+
+template mbc_status Solver::solve_plain<float>(int, const void *, int32_t, void *, int32_t, const void *, bool,
+                                               const mbc_solve_options &, mbc_solve_stats *, int32_t *, cudaStream_t);
+template mbc_status Solver::solve_plain<double>(int, const void *, int32_t, void *, int32_t, const void *, bool,
+                                                const mbc_solve_options &, mbc_solve_stats *, int32_t *, cudaStream_t);
+
+mbc_status Solver::solve(int R, const void *rhs, int32_t rhs_dt, void *X, int32_t x_dt, const void *X0,
+                         bool adjoint, const mbc_solve_options &o, mbc_solve_stats *stats,
+                         int32_t *iters_host, cudaStream_t st)
+{
+  if (!factored) return fail(MBC_BAD_ARG, "solver is not factored (call mbc_solver_factor)");
+  const auto t0 = std::chrono::steady_clock::now();
+  const int64_t launches0 = launches;
+  profile = o.profile != 0;
+  prof_ms_all.clear();
+  mbc_status rs;
+  if (o.schedule == MBC_SCHED_PER_RHS && R > 1) {
+    // one cold-started PCG per column, in order (mfs_torch_ops.cu:166-171)
+    const size_t rows = adjoint ? (size_t)n : (size_t)nf;
+    const size_t ein = rhs_dt == MBC_F64 ? 8 : 4, eout = x_dt == MBC_F64 ? 8 : 4;
+    MBC_TRY(colbuf.reserve(rows * ein + (size_t)n * eout * 2));
+    char *cin = (char *)colbuf.ptr;
+    char *cx0 = cin + rows * ein;
+    char *cout = cx0 + (size_t)n * eout;
+    mbc_solve_stats agg{};
+    agg.true_relres_max = -1;
+    int worst = 0;
+    rs = MBC_OK;
+    for (int c = 0; c < R; ++c) {
+      MBC_CK(cudaMemcpy2DAsync(cin, ein, (const char *)rhs + c * ein, ein * R, ein, rows,
+                               cudaMemcpyDeviceToDevice, st));
+      if (X0)
+        MBC_CK(cudaMemcpy2DAsync(cx0, eout, (const char *)X0 + c * eout, eout * R, eout, n,
+                                 cudaMemcpyDeviceToDevice, st));
+      mbc_solve_stats s1{};
+      int32_t it1 = 0;
+      mbc_solve_options o1 = o;
+      if (precision == MBC_F64 || o.max_refine <= 0)
+        rs = precision == MBC_F64
+                 ? solve_plain<double>(1, cin, rhs_dt, cout, x_dt, X0 ? cx0 : nullptr, adjoint, o1, &s1, &it1, st)
+                 : solve_plain<float>(1, cin, rhs_dt, cout, x_dt, X0 ? cx0 : nullptr, adjoint, o1, &s1, &it1, st);
+      else
+        rs = solve_mixed(1, cin, rhs_dt, cout, x_dt, X0 ? cx0 : nullptr, adjoint, o1, &s1, &it1, st);
+      if (rs != MBC_OK) return rs;
+      MBC_CK(cudaMemcpy2DAsync((char *)X + c * eout, eout * R, cout, eout, eout, n,
+                               cudaMemcpyDeviceToDevice, st));
+      if (iters_host) iters_host[c] = it1;
+      agg.iters_max = std::max(agg.iters_max, s1.iters_max);
+      agg.iters_total += s1.iters_total;
+      agg.n_converged += s1.n_converged;
+      agg.relres_max = std::max(agg.relres_max, s1.relres_max);
+      agg.true_relres_max = std::max(agg.true_relres_max, s1.true_relres_max);
+      agg.refinements = std::max(agg.refinements, s1.refinements);
+      worst = std::max(worst, s1.status_per_worst);
+    }
+    agg.status_per_worst = worst;
+    MBC_CK(cudaStreamSynchronize(st));
+    if (stats) *stats = agg;
+  } else if (precision == MBC_F64) {
+    rs = solve_plain<double>(R, rhs, rhs_dt, X, x_dt, X0, adjoint, o, stats, iters_host, st);
+  } else if (o.max_refine <= 0) {
+    rs = solve_plain<float>(R, rhs, rhs_dt, X, x_dt, X0, adjoint, o, stats, iters_host, st);
+  } else {
+    rs = solve_mixed(R, rhs, rhs_dt, X, x_dt, X0, adjoint, o, stats, iters_host, st);
+  }
+  if (rs != MBC_OK) return rs;
+  if (stats) {
+    stats->t_solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    stats->kernel_launches = launches - launches0;
+    stats->t_matvec_ms = 0;
+    stats->n_matvec = 0;
+    if (profile) {
+      // a matvec pair whose kernels exited on the done flag takes a few
+      // microseconds; count only pairs that did work (> 1% of the longest)
+      float mx = 0.f;
+      for (float v : prof_ms_all) mx = std::max(mx, v);
+      for (float v : prof_ms_all)
+        if (v > 0.01f * mx) {
+          stats->t_matvec_ms += v;
+          stats->n_matvec += 2;
+        }
+    }
+  }
+  if (stats && stats->status_per_worst == 2) return fail(MBC_BREAKDOWN, "PCG breakdown (p.Ap <= 0 or NaN)");
+  if (stats && stats->status_per_worst == 1) return fail(MBC_NOT_CONVERGED, "PCG reached max_iters above tol");
+  return MBC_OK;
+}
+
+}  // namespace mbc
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+using mbc::fail;
+
+struct mbc_solver {
+  mbc::Solver s;
+};
+
+extern "C" mbc_status mbc_solver_create(const mbc_plan *plan, const mbc_operator *op, int32_t precision,
+                                        mbc_stream stream, mbc_solver **out)
+{
+  if (!out) return fail(MBC_BAD_ARG, "out is NULL");
+  *out = nullptr;
+  if (!plan || !op) return fail(MBC_BAD_ARG, "NULL plan or operator");
+  if (precision != MBC_F64 && precision != MBC_F32) return fail(MBC_BAD_ARG, "precision must be MBC_F64 or MBC_F32");
+  if (op->n != plan->p.n || op->nf <= 0) return fail(MBC_BAD_ARG, "operator columns must equal the plan's points");
+  if (op->kind == MBC_OP_DENSE) {
+    if (!op->M || op->ldm < op->n) return fail(MBC_BAD_ARG, "dense operator needs M with ldm >= n");
+  } else if (op->kind == MBC_OP_POINT_KERNEL) {
+    if (!op->x || !op->nx || !op->y) return fail(MBC_BAD_ARG, "point kernel needs x, nx and y");
+  } else {
+    return fail(MBC_BAD_ARG, "unknown operator kind");
+  }
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) {
+    cudaGetLastError();
+    return fail(MBC_CUDA_ERROR, "no CUDA device");
+  }
+  std::unique_ptr<mbc_solver> sv(new (std::nothrow) mbc_solver());
+  if (!sv) return fail(MBC_NO_MEMORY, "solver allocation failed");
+  if (cudaMallocHost((void **)&sv->s.h_flag, sizeof(int32_t) * 4) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MBC_NO_MEMORY, "pinned flag allocation failed");
+  }
+  mbc_status s = sv->s.create(plan->p, *op, precision, (cudaStream_t)stream);
+  if (s != MBC_OK) return s;
+  *out = sv.release();
+  return MBC_OK;
+}
+
+mbc::Solver::~Solver()
+{
+  if (h_flag) cudaFreeHost(h_flag);
+  for (cudaEvent_t e : events) cudaEventDestroy(e);
+}
+
+mbc_status mbc::Solver::ensure_events(int count)
+{
+  while ((int)events.size() < count) {
+    cudaEvent_t e;
+    MBC_CK(cudaEventCreate(&e));
+    events.push_back(e);
+  }
+  return MBC_OK;
+}
+
+extern "C" mbc_status mbc_solver_destroy(mbc_solver *s)
+{
+  delete s;
+  return MBC_OK;
+}
+
+extern "C" mbc_status mbc_solver_factor(mbc_solver *s, mbc_stream stream)
+{
+  if (!s) return fail(MBC_BAD_ARG, "NULL solver");
+  return s->s.factor((cudaStream_t)stream);
+}
+
+extern "C" mbc_status mbc_solver_get_factor(const mbc_solver *s, double *lval_host, double *theta_host)
+{
+  if (!s) return fail(MBC_BAD_ARG, "NULL solver");
+  const mbc::Solver &S = s->s;
+  if (!S.factored) return fail(MBC_BAD_ARG, "solver is not factored");
+  const mbc::Plan &p = *S.plan;
+  const size_t ln = (size_t)p.lptr.back(), tn = (size_t)p.th_ptr.back();
+  auto fetch = [&](const void *src, size_t cnt, double *dst) -> mbc_status {
+    if (S.precision == MBC_F64) {
+      MBC_CK(cudaMemcpy(dst, src, cnt * sizeof(double), cudaMemcpyDeviceToHost));
+    } else {
+      std::vector<float> tmp(cnt);
+      MBC_CK(cudaMemcpy(tmp.data(), src, cnt * sizeof(float), cudaMemcpyDeviceToHost));
+      for (size_t k = 0; k < cnt; ++k) dst[k] = tmp[k];
+    }
+    return MBC_OK;
+  };
+  if (lval_host) MBC_TRY(fetch(S.lval.ptr, ln, lval_host));
+  if (theta_host) MBC_TRY(fetch(S.theta.ptr, tn, theta_host));
+  return MBC_OK;
+}
+
+extern "C" mbc_status mbc_solver_get_pivot_retries(const mbc_solver *s, int32_t *count)
+{
+  if (!s || !count) return fail(MBC_BAD_ARG, "NULL argument");
+  *count = s->s.pivot_retries;
+  return MBC_OK;
+}
+
+extern "C" void mbc_solve_default_options(mbc_solve_options *o)
+{
+  if (!o) return;
+  o->max_iters = 1000;
+  o->tol = 1e-8;
+  o->schedule = MBC_SCHED_BATCHED;
+  o->precondition = 1;
+  o->max_refine = 4;
+  o->inner_tol = 1e-4;
+  o->check_every = 8;
+  o->true_residual = 0;
+}
+
+static mbc_status check_solve_args(mbc_solver *s, int32_t R, const void *in, int32_t in_dt, void *X,
+                                   int32_t x_dt)
+{
+  if (!s) return fail(MBC_BAD_ARG, "NULL solver");
+  if (R <= 0 || !in || !X) return fail(MBC_BAD_ARG, "need R > 0 and device arrays");
+  if ((in_dt != MBC_F64 && in_dt != MBC_F32) || (x_dt != MBC_F64 && x_dt != MBC_F32))
+    return fail(MBC_BAD_ARG, "dtype must be MBC_F64 or MBC_F32");
+  return MBC_OK;
+}
+
+extern "C" mbc_status mbc_solve(mbc_solver *s, int32_t R, const void *F, int32_t f_dtype, void *X,
+                                int32_t x_dtype, const void *X0, const mbc_solve_options *opt,
+                                mbc_solve_stats *stats_host, int32_t *iters_host, mbc_stream stream)
+{
+  MBC_TRY(check_solve_args(s, R, F, f_dtype, X, x_dtype));
+  mbc_solve_options o;
+  mbc_solve_default_options(&o);
+  if (opt) o = *opt;
+  if (o.max_iters < 0 || !(o.tol >= 0)) return fail(MBC_BAD_ARG, "bad solve options");
+  return s->s.solve(R, F, f_dtype, X, x_dtype, X0, false, o, stats_host, iters_host, (cudaStream_t)stream);
+}
+
+extern "C" mbc_status mbc_solve_adjoint(mbc_solver *s, int32_t R, const void *B, int32_t b_dtype, void *X,
+                                        int32_t x_dtype, const mbc_solve_options *opt,
+                                        mbc_solve_stats *stats_host, int32_t *iters_host, mbc_stream stream)
+{
+  MBC_TRY(check_solve_args(s, R, B, b_dtype, X, x_dtype));
+  mbc_solve_options o;
+  mbc_solve_default_options(&o);
+  if (opt) o = *opt;
+  if (o.max_iters < 0 || !(o.tol >= 0)) return fail(MBC_BAD_ARG, "bad solve options");
+  return s->s.solve(R, B, b_dtype, X, x_dtype, nullptr, true, o, stats_host, iters_host, (cudaStream_t)stream);
+}
+
+extern "C" mbc_status mbc_apply_K(mbc_solver *s, int32_t R, const void *V, void *W, mbc_stream stream)
+{
+  if (!s || R <= 0 || !V || !W) return fail(MBC_BAD_ARG, "bad arguments");
+  mbc::Solver &S = s->s;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (S.precision == MBC_F64) {
+    MBC_TRY(S.tmp.reserve(sizeof(double) * (size_t)S.n * R));
+    mbc::permute_in<double>(S, R, V, MBC_F64, (double *)S.tmp.ptr, st);
+    mbc::launch_rows<double>(S, R, (const double *)S.tmp.ptr, (double *)W, nullptr, st);
+  } else {
+    MBC_TRY(S.tmp.reserve(sizeof(float) * (size_t)S.n * R));
+    mbc::permute_in<float>(S, R, V, MBC_F32, (float *)S.tmp.ptr, st);
+    mbc::launch_rows<float>(S, R, (const float *)S.tmp.ptr, (float *)W, nullptr, st);
+  }
+  MBC_CKL();
+  MBC_CK(cudaStreamSynchronize(st));
+  return MBC_OK;
+}
+
+extern "C" mbc_status mbc_apply_KT(mbc_solver *s, int32_t R, const void *W, void *T, mbc_stream stream)
+{
+  if (!s || R <= 0 || !W || !T) return fail(MBC_BAD_ARG, "bad arguments");
+  mbc::Solver &S = s->s;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (S.precision == MBC_F64) {
+    MBC_TRY(S.tmp.reserve(sizeof(double) * (size_t)S.n * R));
+    mbc::launch_cols<double>(S, R, (const double *)W, (double *)S.tmp.ptr, nullptr, nullptr, nullptr, st);
+    mbc::permute_out<double>(S, R, (const double *)S.tmp.ptr, T, MBC_F64, st);
+  } else {
+    MBC_TRY(S.tmp.reserve(sizeof(float) * (size_t)S.n * R));
+    mbc::launch_cols<float>(S, R, (const float *)W, (float *)S.tmp.ptr, nullptr, nullptr, nullptr, st);
+    mbc::permute_out<float>(S, R, (const float *)S.tmp.ptr, T, MBC_F32, st);
+  }
+  MBC_CKL();
+  MBC_CK(cudaStreamSynchronize(st));
+  return MBC_OK;
+}

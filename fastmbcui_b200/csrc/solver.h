@@ -1,0 +1,89 @@
+// Device solver object behind mbc_solver.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "mbc_internal.h"
+
+namespace mbc {
+
+// Owned device allocation that only grows.
+struct DevMem {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  DevMem() = default;
+  DevMem(const DevMem &) = delete;
+  DevMem &operator=(const DevMem &) = delete;
+  ~DevMem();
+  mbc_status reserve(size_t b);
+  void release();
+};
+
+struct Solver {
+  const Plan *plan = nullptr;
+  mbc_operator op{};
+  int32_t precision = MBC_F64;
+  int32_t n = 0, nf = 0;
+  bool factored = false;
+  int32_t pivot_retries = 0;
+  int32_t *h_flag = nullptr;  // pinned
+  int64_t launches = 0;       // kernels launched by this solver (solve paths)
+  bool profile = false;
+  std::vector<cudaEvent_t> events;
+  std::vector<float> prof_ms_all;
+
+  // plan on the device
+  DevMem m_P, m_Pinv, m_sup_ptr, m_sup_ind, m_set_ptr, m_set_ind, m_lptr, m_lind, m_rptr, m_rcol,
+      m_rmap, m_th_ptr;
+  DevMem class_list[4];
+  // operator: rows (original order) and sources (new order) as float4
+  DevMem m_x4, m_n4, m_y4;
+  // factor
+  DevMem theta, theta64, lval, bad, fscratch;
+  // PCG workspaces
+  DevMem work32, work64, part, scal, fbuf32, fbuf64, res64, mask, colbuf, tmp, b2ref, nrm;
+
+  ~Solver();
+
+  const int32_t *dP() const { return (const int32_t *)m_P.ptr; }
+  const int32_t *d_Pinv() const { return (const int32_t *)m_Pinv.ptr; }
+  const int32_t *d_sup_ptr() const { return (const int32_t *)m_sup_ptr.ptr; }
+  const int32_t *d_sup_ind() const { return (const int32_t *)m_sup_ind.ptr; }
+  const int32_t *d_set_ptr() const { return (const int32_t *)m_set_ptr.ptr; }
+  const int32_t *d_set_ind() const { return (const int32_t *)m_set_ind.ptr; }
+  const int32_t *d_lptr() const { return (const int32_t *)m_lptr.ptr; }
+  const int32_t *d_lind() const { return (const int32_t *)m_lind.ptr; }
+  const int32_t *d_rptr() const { return (const int32_t *)m_rptr.ptr; }
+  const int32_t *d_rcol() const { return (const int32_t *)m_rcol.ptr; }
+  const int32_t *d_rmap() const { return (const int32_t *)m_rmap.ptr; }
+  const int64_t *d_th_ptr() const { return (const int64_t *)m_th_ptr.ptr; }
+  const float4 *x4() const { return (const float4 *)m_x4.ptr; }
+  const float4 *n4() const { return (const float4 *)m_n4.ptr; }
+  const float4 *y4() const { return (const float4 *)m_y4.ptr; }
+
+  mbc_status create(const Plan &pl, const mbc_operator &o, int32_t prec, cudaStream_t st);
+  mbc_status ensure_events(int count);
+  mbc_status factor(cudaStream_t st);
+  mbc_status solve(int R, const void *rhs, int32_t rhs_dt, void *X, int32_t x_dt, const void *X0,
+                   bool adjoint, const mbc_solve_options &o, mbc_solve_stats *stats,
+                   int32_t *iters_host, cudaStream_t st);
+  template <typename T>
+  mbc_status solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, int32_t x_dt,
+                         const void *X0, bool adjoint, const mbc_solve_options &o,
+                         mbc_solve_stats *stats, int32_t *iters_host, cudaStream_t st);
+  mbc_status solve_mixed(int R, const void *rhs, int32_t rhs_dt, void *X, int32_t x_dt,
+                         const void *X0, bool adjoint, const mbc_solve_options &o,
+                         mbc_solve_stats *stats, int32_t *iters_host, cudaStream_t st);
+  mbc_status true_residual(int R, const void *F, int32_t f_dt, const void *X, int32_t x_dt,
+                           mbc_solve_stats *stats, cudaStream_t st);
+};
+
+template <typename T>
+void launch_rows(const Solver &S, int R, const T *v, T *w, const int32_t *done, cudaStream_t st);
+template <typename T>
+int launch_cols(const Solver &S, int R, const T *w, T *t, const T *pdot, double *part,
+                const int32_t *done, cudaStream_t st);
+
+}  // namespace mbc

@@ -1,0 +1,220 @@
+/*
+ * mbc.h -- C ABI of the B200-native MFS solve path (libmbc.so).
+ *
+ * The path: maximin ordering -> KL sparsity pattern -> supernodes (host C++,
+ * bit-exact to the reference), supernodal KL-Cholesky factor of (K^T K)^-1
+ * and PCG on the normal equations (CUDA, sm_100a).  K is the MFS collocation
+ * operator: a caller-provided dense matrix (the mfs_torch operator's input) or
+ * the Laplace point kernel evaluated on the fly.
+ *
+ * Conventions
+ *   - Every function returns mbc_status and never exits the process.
+ *     mbc_last_error() gives a message for the calling thread.
+ *   - Arrays named *_host live in host memory; every other array pointer is a
+ *     device pointer on the current CUDA device.
+ *   - Matrices are row-major.  A "source-space" array (n x R) is indexed by the
+ *     ORIGINAL source order unless its name says otherwise.
+ *   - mbc_stream is cudaStream_t; NULL is the legacy default stream.
+ *   - Objects are caller-owned; the library keeps no global state.
+ */
+#ifndef MBC_H
+#define MBC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *mbc_stream;
+
+typedef enum {
+  MBC_OK = 0,
+  MBC_NOT_CONVERGED = 1, /* max iterations reached above the tolerance */
+  MBC_BREAKDOWN = 2,     /* PCG curvature p.Ap <= 0 or NaN */
+  MBC_NONSPD_PIVOT = 3,  /* a supernode Cholesky pivot was <= 0 even after the FP64 retry */
+  MBC_BAD_ARG = 4,
+  MBC_CUDA_ERROR = 5,
+  MBC_TIMEOUT = 6,       /* a bounded device wait gave up */
+  MBC_NO_MEMORY = 7,
+  MBC_COVERAGE = 8,      /* aggregation did not cover every point (e.g. duplicate points) */
+  MBC_UNSUPPORTED = 9
+} mbc_status;
+
+typedef enum { MBC_F64 = 0, MBC_F32 = 1 } mbc_dtype;
+
+const char *mbc_status_string(mbc_status s);
+const char *mbc_last_error(void);
+/* Library version as 10000*major + 100*minor + patch. */
+int32_t mbc_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Plan: ordering, pattern, supernodes (host).                               */
+/* Replaces klchol::fps_sampler (src/preprocess.h:17-671): fps_sampler(pts), */
+/* compute('F'), P(), simpl_sparsity(rho, 1, PATT), aggregate(1, {0,N},      */
+/* PATT, lambda, ..., max_super), super_sparsity(1, PATT, parent, SUP_PATT), */
+/* as called by mfs_torch/csrc/mfs_torch_ops.cu:51-55 and :114-116.          */
+/* ------------------------------------------------------------------------ */
+typedef struct mbc_plan mbc_plan;
+
+typedef struct {
+  double rho;        /* pattern radius factor; used as (double)(float)rho (mfs_torch_ops.cu:114) */
+  double lambda;     /* supernode scale ratio, 1.5 in the reference */
+  int32_t max_super; /* max columns per supernode, 2048 in the reference */
+  int32_t n_threads; /* host threads for the pattern; 0 = all */
+} mbc_plan_options;
+
+typedef struct {
+  int32_t n;
+  int32_t n_super;
+  int64_t pattern_nnz;
+  int64_t factor_nnz;
+  int64_t theta_nnz;  /* sum over supernodes of n_s^2 */
+  int32_t max_set;    /* largest supernode row set */
+  int32_t root;       /* original index of the first (coarsest) point */
+  double t_order_ms, t_pattern_ms, t_super_ms;
+} mbc_plan_info;
+
+void mbc_plan_default_options(mbc_plan_options *opt);
+/* pts_host: n x 3 (double).  The mfs_torch operator widens float32 points. */
+mbc_status mbc_plan_create(int32_t n, const double *pts_host, const mbc_plan_options *opt,
+                           mbc_plan **out);
+mbc_status mbc_plan_destroy(mbc_plan *plan);
+mbc_status mbc_plan_get_info(const mbc_plan *plan, mbc_plan_info *info);
+/* P[orig] = position in the fine-to-coarse order; scale in that order. */
+mbc_status mbc_plan_get_order(const mbc_plan *plan, int32_t *P_host, double *scale_host);
+/* MRA pattern, CSC over the new order: ptr[n+1], ind[pattern_nnz]. */
+mbc_status mbc_plan_get_pattern(const mbc_plan *plan, int32_t *ptr_host, int32_t *ind_host);
+mbc_status mbc_plan_get_supernodes(const mbc_plan *plan, int32_t *sup_ptr_host,
+                                   int32_t *sup_ind_host, int32_t *sup_parent_host);
+/* Supernodal factor pattern, CSC: lptr[n+1], lind[factor_nnz]. */
+mbc_status mbc_plan_get_factor_pattern(const mbc_plan *plan, int32_t *lptr_host,
+                                       int32_t *lind_host);
+
+/* ------------------------------------------------------------------------ */
+/* Operator K (nf collocation rows x n source columns).                       */
+/* ------------------------------------------------------------------------ */
+typedef enum { MBC_OP_DENSE = 0, MBC_OP_POINT_KERNEL = 1 } mbc_op_kind;
+
+typedef struct {
+  int32_t kind;
+  int32_t nf, n;
+  /* MBC_OP_DENSE: row-major nf x n float32, row stride ldm (>= n). */
+  const float *M;
+  int64_t ldm;
+  /* MBC_OP_POINT_KERNEL: K(i,j) = coef ((x_i - y_j).n_i) / |x_i - y_j|^3
+   * (src/kernels.h:24-40 with coef = 1).  x, nx: nf x 3; y: n x 3. */
+  const float *x, *nx, *y;
+  double coef;
+} mbc_operator;
+
+/* ------------------------------------------------------------------------ */
+/* Solver: device factor + PCG.                                               */
+/* Replaces klchol::gpu_super_klchol (src/kl_chol.h:143-336): set_kernel,    */
+/* build_cov_mat_LS_float, set_supernodes, set_sppatt, compute, pcg_guesss,   */
+/* pcg_VpL_guesss, get_TH_val / get_val.                                     */
+/* ------------------------------------------------------------------------ */
+typedef struct mbc_solver mbc_solver;
+
+/* precision MBC_F64: the plain method, FP64 throughout.
+ * precision MBC_F32: matvec, factor and preconditioner in FP32; PCG scalars,
+ * dot products and the true residual in FP64 with iterative refinement. */
+mbc_status mbc_solver_create(const mbc_plan *plan, const mbc_operator *op, int32_t precision,
+                             mbc_stream stream, mbc_solver **out);
+mbc_status mbc_solver_destroy(mbc_solver *s);
+/* Assemble Theta, factor every supernode, form the KL columns (kl_chol.cu:772-812). */
+mbc_status mbc_solver_factor(mbc_solver *s, mbc_stream stream);
+/* Copy the factor out for parity checks: lval[factor_nnz] (CSC of the plan),
+ * theta[theta_nnz] (per supernode, reversed, column-major, U in the upper part;
+ * NULL to skip).  Values are widened to double. */
+mbc_status mbc_solver_get_factor(const mbc_solver *s, double *lval_host, double *theta_host);
+/* Number of supernodes whose Cholesky needed the FP64 diagonal-shift retry. */
+mbc_status mbc_solver_get_pivot_retries(const mbc_solver *s, int32_t *count);
+
+typedef enum {
+  MBC_SCHED_BATCHED = 0, /* all R columns advance together (per-column alpha, beta, stop) */
+  MBC_SCHED_PER_RHS = 1  /* one cold-started PCG per column, in order (the reference's loop) */
+} mbc_schedule;
+
+typedef struct {
+  int32_t max_iters;     /* per column (per refinement sweep in MBC_F32) */
+  double tol;            /* stop when |r|^2 < tol^2 |b|^2, b = K^T f (kl_chol.cu:955) */
+  int32_t schedule;      /* mbc_schedule */
+  int32_t precondition;  /* 1 = KL preconditioner (the reference always passes true) */
+  int32_t max_refine;    /* MBC_F32: outer FP64 refinement sweeps (>= 1) */
+  double inner_tol;      /* MBC_F32: relative tolerance of each inner sweep */
+  int32_t check_every;   /* iterations between convergence checks on the host */
+  int32_t true_residual; /* 1 = report the FP64-recomputed |K^T(f-Kx)|/|K^T f| */
+  int32_t profile;       /* 1 = time the matvec kernels with CUDA events on `stream` */
+} mbc_solve_options;
+
+typedef struct {
+  int32_t status_per_worst; /* worst per-column status */
+  int32_t iters_max;        /* most iterations any column took */
+  int64_t iters_total;      /* summed over columns */
+  int32_t refinements;      /* outer sweeps done (MBC_F32) */
+  int32_t n_converged;
+  double relres_max;        /* recursive residual (or true one when requested) */
+  double true_relres_max;   /* FP64 |K^T(f-Kx)|/|K^T f|, if requested, else -1 */
+  double t_solve_ms;
+  double t_matvec_ms;       /* profile: summed duration of the K and K^T kernels */
+  int64_t n_matvec;         /* profile: K / K^T launches timed */
+  int64_t kernel_launches;  /* kernels this call launched */
+} mbc_solve_stats;
+
+void mbc_solve_default_options(mbc_solve_options *opt);
+
+/* Forward solve (kl_chol.cu:891-1088, per column of F):
+ *   min |K x - f|  via  (K^T K) x = K^T f.
+ * F: nf x R, X: n x R (ORIGINAL source order), element type f_dtype / x_dtype.
+ * X0: NULL for a cold start (x0 = 0), else an n x R warm start (x_dtype).
+ * iters_host: optional int32[R]. */
+mbc_status mbc_solve(mbc_solver *s, int32_t R, const void *F, int32_t f_dtype, void *X,
+                     int32_t x_dtype, const void *X0, const mbc_solve_options *opt,
+                     mbc_solve_stats *stats_host, int32_t *iters_host, mbc_stream stream);
+
+/* Adjoint solve (kl_chol.cu:1090-1264): (K^T K) x = b, B: n x R, ORIGINAL order. */
+mbc_status mbc_solve_adjoint(mbc_solver *s, int32_t R, const void *B, int32_t b_dtype, void *X,
+                             int32_t x_dtype, const mbc_solve_options *opt,
+                             mbc_solve_stats *stats_host, int32_t *iters_host,
+                             mbc_stream stream);
+
+/* Operator applications in the ORIGINAL source order, for checks:
+ * W (nf x R) = K V (n x R);  T (n x R) = K^T W.  dtype of V/W/T = precision. */
+mbc_status mbc_apply_K(mbc_solver *s, int32_t R, const void *V, void *W, mbc_stream stream);
+mbc_status mbc_apply_KT(mbc_solver *s, int32_t R, const void *W, void *T, mbc_stream stream);
+
+/* ------------------------------------------------------------------------ */
+/* mfs_torch operator bodies (the drop-in).                                   */
+/* mbc_minvf_float replaces MinvF_float (mfs_torch/csrc/mfs_torch_ops.cu:21-197, */
+/* registered as mfs_torch::MinvF_float_fastGrad, mfs_torch_ops.cpp:9);       */
+/* mbc_vpl_fast_float replaces VpL_fast_float (mfs_torch_ops.cu:199-370,      */
+/* mfs_torch_ops.cpp:8).  The context replaces the op's process-wide static  */
+/* factor cache (mfs_torch_ops.cu:17-19): the adjoint reuses the factor of    */
+/* the last forward on the same points and M, and refactors otherwise.        */
+/*   M: device nf x n float32 row-major; F: device nf x R; pL: device n x R;  */
+/*   Vs_host: host n x 3 float32; out: device n x R float32 (original order).  */
+/* ------------------------------------------------------------------------ */
+typedef struct mbc_context mbc_context;
+
+mbc_status mbc_context_create(mbc_context **out);
+mbc_status mbc_context_destroy(mbc_context *ctx);
+/* Iterations / residual of the last call through this context. */
+mbc_status mbc_context_last_stats(const mbc_context *ctx, mbc_solve_stats *stats_host);
+
+mbc_status mbc_minvf_float(mbc_context *ctx, const float *M, int32_t nf, int32_t n,
+                           const float *F, int32_t R, const float *Vs_host, double rho,
+                           int64_t pcg_max_iter, double tol_r, int32_t timing_verbose,
+                           int32_t solve_verbose, float *out, mbc_stream stream);
+
+mbc_status mbc_vpl_fast_float(mbc_context *ctx, const float *M, int32_t nf, int32_t n,
+                              const float *pL, int32_t R, const float *Vs_host, double rho,
+                              int64_t pcg_max_iter, double tol_r, int32_t timing_verbose,
+                              int32_t solve_verbose, float *out, mbc_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MBC_H */

@@ -1,0 +1,248 @@
+"""GPU parity: libmbc's CUDA path against the FP64 CPU oracle.
+
+Tolerances (stated per check):
+  * matvec K, K^T: FP64 path 1e-12 relative (norm-wise), FP32 path 2e-5;
+  * KL factor values: FP64 path 1e-7 relative per column, FP32 path 2e-2;
+  * PCG: iteration counts within 2 of the oracle's (same algorithm, FP64),
+    fitted flux K x within 1e-6 of the oracle's (relative to |f|), and the
+    FP64-recomputed normal-equation residual at or below the tolerance;
+  * strengths x themselves are ill-conditioned, so they are compared only
+    after both sides solve to 1e-12, within 1e-5.
+"""
+import numpy as np
+import pytest
+
+import fastmbcui_b200 as F
+import oracle as O
+from fastmbcui_b200 import scenes as S
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _dev(a, dt=torch.float32):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device="cuda")
+
+
+class Case:
+    def __init__(self, sc):
+        self.sc = sc
+        self.op = O.Op.from_scene(sc)
+        self.pl = O.plan(sc.y, sc.rho, sc.lam, sc.max_super)
+        self.th, self.lval, self.bad = O.factor(self.op, self.pl)
+        self.plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
+        self.x = _dev(sc.x)
+        self.nx = _dev(sc.nx)
+        self.y = _dev(sc.y)
+
+    def solver(self, prec):
+        s = F.Solver(self.plan, x=self.x, nx=self.nx, y=self.y, coef=self.sc.coef, precision=prec)
+        return s.factor()
+
+    def true_relres(self, X, Fm):
+        X = np.atleast_2d(np.asarray(X, np.float64).T).T
+        Fm = np.atleast_2d(Fm.T).T
+        r = self.op.KT(Fm - self.op.K(X))
+        b = self.op.KT(Fm)
+        nb = np.linalg.norm(b, axis=0)
+        return np.where(nb > 1e-8, np.linalg.norm(r, axis=0) / np.maximum(nb, 1e-300), 0.0)
+
+
+@pytest.fixture(scope="module")
+def sphere():
+    return Case(S.sphere_scene())
+
+
+@pytest.fixture(scope="module")
+def ells():
+    return Case(S.ellipsoids_scene(2, 1500, seed=21))
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300)
+
+
+@pytest.mark.parametrize("prec,tol", [(F.MBC_F64, 1e-12), (F.MBC_F32, 2e-5)])
+@pytest.mark.parametrize("R", [1, 3, 8, 40, 96])
+def test_point_kernel_matvec(sphere, prec, tol, R):
+    s = sphere.solver(prec)
+    dt = torch.float64 if prec == F.MBC_F64 else torch.float32
+    rng = np.random.default_rng(R)
+    V = rng.standard_normal((sphere.sc.n, R))
+    W = rng.standard_normal((sphere.sc.nf, R))
+    if dt == torch.float32:
+        V, W = V.astype(np.float32).astype(np.float64), W.astype(np.float32).astype(np.float64)
+    got_K = s.apply_K(_dev(V, dt)).cpu().numpy()
+    got_KT = s.apply_KT(_dev(W, dt)).cpu().numpy()
+    assert rel(got_K, sphere.op.K(V)) < tol
+    assert rel(got_KT, sphere.op.KT(W)) < tol
+
+
+@pytest.mark.parametrize("R", [1, 5, 33])
+def test_dense_matvec(ells, R):
+    K32 = ells.sc.dense_K().astype(np.float32)
+    s = F.Solver(ells.plan, M=_dev(K32), precision=F.MBC_F64).factor()
+    rng = np.random.default_rng(1)
+    V = rng.standard_normal((ells.sc.n, R))
+    W = rng.standard_normal((ells.sc.nf, R))
+    K64 = K32.astype(np.float64)
+    assert rel(s.apply_K(_dev(V, torch.float64)).cpu().numpy(), K64 @ V) < 1e-12
+    assert rel(s.apply_KT(_dev(W, torch.float64)).cpu().numpy(), K64.T @ W) < 1e-12
+
+
+def _column_rel(a, b, lptr):
+    worst = 0.0
+    for j in range(len(lptr) - 1):
+        sl = slice(lptr[j], lptr[j + 1])
+        worst = max(worst, rel(a[sl], b[sl]))
+    return worst
+
+
+@pytest.mark.parametrize("case", ["sphere", "ells"])
+def test_factor_f64_matches_oracle(case, request):
+    c = request.getfixturevalue(case)
+    s = c.solver(F.MBC_F64)
+    lval, theta = s.get_factor(theta=True)
+    assert c.bad == 0 and s.pivot_retries() == 0
+    assert _column_rel(lval, c.lval, c.pl["lptr"]) < 1e-7
+    # the factored Theta: U in the upper part of each reversed block
+    tp, sp = c.pl["th_ptr"], c.pl["set_ptr"]
+    for sn in range(0, c.pl["n_super"], max(1, c.pl["n_super"] // 25)):
+        ns = sp[sn + 1] - sp[sn]
+        A = theta[tp[sn]:tp[sn + 1]].reshape(ns, ns).T
+        B = c.th[tp[sn]:tp[sn + 1]].reshape(ns, ns).T
+        assert rel(np.triu(A), np.triu(B)) < 1e-7
+        assert rel(np.tril(A, -1), np.tril(B, -1)) < 1e-12
+
+
+def test_factor_dense_operator_matches_point_kernel(ells):
+    K32 = ells.sc.dense_K().astype(np.float32)
+    s = F.Solver(ells.plan, M=_dev(K32), precision=F.MBC_F64).factor()
+    op = O.Op(ells.sc.nf, ells.sc.n, M=K32.astype(np.float64))
+    _, lval_o, _ = O.factor(op, ells.pl)
+    lval, _ = s.get_factor()
+    assert _column_rel(lval, lval_o, ells.pl["lptr"]) < 1e-7
+
+
+def test_factor_f32_close(sphere):
+    s = sphere.solver(F.MBC_F32)
+    lval, _ = s.get_factor()
+    assert _column_rel(lval, sphere.lval, sphere.pl["lptr"]) < 2e-2
+
+
+def test_pcg_f64_matches_oracle(sphere):
+    Fm = sphere.sc.rhs()[:, :3]
+    s = sphere.solver(F.MBC_F64)
+    X, st, its = s.solve(_dev(Fm, torch.float64), iters=True, tol=1e-8, max_iters=2000,
+                         true_residual=1)
+    X = X.cpu().numpy()
+    for c in range(3):
+        xo, it, rr = O.pcg(sphere.op, sphere.pl, sphere.lval, f=Fm[:, c], maxits=2000, tol=1e-8)
+        assert abs(int(its[c]) - it) <= 2, (its[c], it)
+        flux = sphere.op.K(X[:, c])
+        flux_o = sphere.op.K(xo[sphere.pl["P"]])
+        assert np.linalg.norm(flux - flux_o) / np.linalg.norm(Fm[:, c]) < 1e-6
+    assert st["n_converged"] == 3
+    assert st["true_relres_max"] <= 1.05e-8
+    assert np.all(sphere.true_relres(X, Fm) <= 1.05e-8)
+
+
+def test_strengths_tight(ells):
+    Fm = ells.sc.rhs()[:, [0, 4]]
+    s = ells.solver(F.MBC_F64)
+    X, st = s.solve(_dev(Fm, torch.float64), tol=1e-12, max_iters=5000)
+    X = X.cpu().numpy()
+    for k in range(2):
+        xo, it, rr = O.pcg(ells.op, ells.pl, ells.lval, f=Fm[:, k], maxits=5000, tol=1e-12)
+        assert rel(X[:, k], xo[ells.pl["P"]]) < 1e-5
+
+
+def test_per_rhs_schedule_equals_batched(ells):
+    Fm = ells.sc.rhs()
+    s = ells.solver(F.MBC_F64)
+    Xb, stb, itb = s.solve(_dev(Fm, torch.float64), iters=True, tol=1e-8, max_iters=3000)
+    Xp, stp, itp = s.solve(_dev(Fm, torch.float64), iters=True, tol=1e-8, max_iters=3000,
+                           schedule=F.MBC_SCHED_PER_RHS)
+    assert np.array_equal(itb, itp)
+    assert rel(Xb.cpu().numpy(), Xp.cpu().numpy()) < 1e-9
+
+
+def test_mixed_precision_reaches_tolerance(ells):
+    Fm = ells.sc.rhs()
+    s = ells.solver(F.MBC_F32)
+    X, st = s.solve(_dev(Fm), out_dtype=torch.float64, tol=1e-8, max_iters=3000, max_refine=6,
+                    inner_tol=1e-4)
+    X = X.cpu().numpy()
+    assert st["n_converged"] == Fm.shape[1], st
+    assert st["true_relres_max"] <= 1e-8
+    tr = ells.true_relres(X, Fm)
+    assert np.all(tr <= 1.2e-8), tr
+    s64 = ells.solver(F.MBC_F64)
+    X64, _ = s64.solve(_dev(Fm, torch.float64), tol=1e-8, max_iters=3000)
+    X64 = X64.cpu().numpy()
+    flux = ells.op.K(X)
+    flux64 = ells.op.K(X64)
+    assert np.linalg.norm(flux - flux64) / np.linalg.norm(Fm) < 1e-6
+
+
+def test_zero_rhs_columns(sphere):
+    # rotations of a sphere about its centre have zero normal velocity
+    Fm = sphere.sc.rhs()
+    s = sphere.solver(F.MBC_F64)
+    X, st, its = s.solve(_dev(Fm, torch.float64), iters=True, tol=1e-8, max_iters=2000)
+    X = X.cpu().numpy()
+    assert np.all(its[3:] == 0) and np.all(X[:, 3:] == 0)
+    assert np.all(its[:3] > 0)
+
+
+def test_warm_start(ells):
+    Fm = ells.sc.rhs()[:, :4]
+    s = ells.solver(F.MBC_F64)
+    X, st, its = s.solve(_dev(Fm, torch.float64), iters=True, tol=1e-8, max_iters=3000)
+    Xw, stw, itw = s.solve(_dev(Fm, torch.float64), X0=X, iters=True, tol=1e-8, max_iters=3000)
+    assert np.all(itw <= 1)
+    noisy = X * (1 + 1e-3 * torch.randn_like(X))
+    Xn, stn, itn = s.solve(_dev(Fm, torch.float64), X0=noisy, iters=True, tol=1e-8, max_iters=3000)
+    assert np.all(itn < its)
+    assert np.all(ells.true_relres(Xn.cpu().numpy(), Fm) <= 1.05e-8)
+
+
+def test_adjoint_matches_oracle(ells):
+    rng = np.random.default_rng(5)
+    B = rng.standard_normal((ells.sc.n, 3))
+    s = ells.solver(F.MBC_F64)
+    X, st, its = s.solve_adjoint(_dev(B, torch.float64), iters=True, tol=1e-10, max_iters=4000)
+    X = X.cpu().numpy()
+    for c in range(3):
+        xo, it, rr = O.pcg(ells.op, ells.pl, ells.lval, b=B[ells.pl["Pinv"], c], maxits=4000, tol=1e-10)
+        assert abs(int(its[c]) - it) <= 2
+        assert rel(ells.op.KT(ells.op.K(X[:, c])), B[:, c]) < 1e-9
+
+
+def test_unpreconditioned_matches_oracle(ells):
+    Fm = ells.sc.rhs()[:, :1]
+    s = ells.solver(F.MBC_F64)
+    X, st, its = s.solve(_dev(Fm, torch.float64), iters=True, tol=1e-6, max_iters=4000, precondition=0)
+    xo, it, rr = O.pcg(ells.op, ells.pl, ells.lval, f=Fm[:, 0], maxits=4000, tol=1e-6, precond=False)
+    assert abs(int(its[0]) - it) <= 2
+
+
+def test_nan_rhs_reports_breakdown(ells):
+    # a fault injected on the host: NaN in the right-hand side
+    Fm = ells.sc.rhs()[:, :2].copy()
+    Fm[5, 1] = np.nan
+    s = ells.solver(F.MBC_F64)
+    with pytest.raises(F.MbcError) as e:
+        s.solve(_dev(Fm, torch.float64), tol=1e-8, max_iters=50)
+    assert e.value.status == 2  # MBC_BREAKDOWN
+
+
+def test_max_iters_reports_not_converged(ells):
+    Fm = ells.sc.rhs()[:, :1]
+    s = ells.solver(F.MBC_F64)
+    with pytest.raises(F.MbcError) as e:
+        s.solve(_dev(Fm, torch.float64), tol=1e-14, max_iters=5, ok_not_converged=False)
+    assert e.value.status == 1
+    X, st, its = s.solve(_dev(Fm, torch.float64), iters=True, tol=1e-14, max_iters=5)
+    assert its[0] == 5

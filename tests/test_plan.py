@@ -1,0 +1,87 @@
+"""Product host plan (libmbc.so, C ABI) equals the oracle bit for bit."""
+import numpy as np
+import pytest
+
+import fastmbcui_b200 as F
+import oracle as O
+from fastmbcui_b200 import scenes as S
+
+KEYS = [("order", ("P", "scale")), ("pattern", ("ptr", "ind")),
+        ("supernodes", ("sup_ptr", "sup_ind", "sup_parent")), ("factor_pattern", ("lptr", "lind"))]
+
+
+def assert_same(y, rho=3.0, lam=1.5, max_super=2048):
+    p = F.Plan(y, rho, lam, max_super)
+    o = O.plan(y, rho, lam, max_super)
+    for meth, names in KEYS:
+        got = getattr(p, meth)()
+        for g, k in zip(got, names):
+            assert np.array_equal(g, o[k]), (meth, k)
+    assert p.info.n_super == o["n_super"]
+    assert p.info.theta_nnz == int(o["th_ptr"][-1])
+    return p, o
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_ellipsoid_scenes(seed):
+    rng = np.random.default_rng(seed)
+    nb = int(rng.integers(1, 5))
+    sc = S.ellipsoids_scene(nb, rng.integers(200, 1500, size=nb), seed=100 + seed)
+    assert_same(sc.y)
+
+
+@pytest.mark.parametrize("rho", [1.15, 1.2, 2.0, 3.0, 4.0, 6.9, 7.0, 9.5])
+def test_rho_branches_and_float_widening(rho):
+    sc = S.coins_scene(n_coins=2, pts=700)
+    assert_same(sc.y, rho=rho)
+
+
+@pytest.mark.parametrize("max_super", [1, 2, 5, 17])
+def test_supernode_cap(max_super):
+    sc = S.sphere_scene(subdiv=3)
+    p, _ = assert_same(sc.y, max_super=max_super)
+    sp, _, _ = p.supernodes()
+    assert np.diff(sp).max() <= max_super
+
+
+@pytest.mark.parametrize("lam", [1.0, 1.5, 3.0])
+def test_lambda(lam):
+    assert_same(S.ellipsoids_scene(2, 600, seed=5).y, lam=lam)
+
+
+def test_sphere_and_ties():
+    assert_same(S.sphere_scene().y)
+    g = np.stack(np.meshgrid(np.arange(10), np.arange(10), np.arange(4)), -1).reshape(-1, 3) * 0.25
+    assert_same(g.astype(np.float64))
+
+
+def test_far_apart_clusters():
+    rng = np.random.default_rng(3)
+    a = np.float32(rng.random((300, 3))).astype(np.float64)
+    y = np.concatenate([a, a + 1000.0, a * 0.01 - 50.0])
+    assert_same(y)
+
+
+def test_two_points():
+    assert_same(np.array([[0.0, 0, 0], [0.5, -1.0, 2.0]]))
+
+
+def test_large_scene_plan():
+    sc = S.ellipsoids_scene(32, 2000, seed=4)
+    p, _ = assert_same(sc.y)
+    assert p.info.n == 64000
+
+
+def test_errors():
+    with pytest.raises(F.MbcError) as e:
+        F.Plan(np.zeros((1, 3)))
+    assert e.value.status == 8  # MBC_COVERAGE: the reference asserts here
+    with pytest.raises(F.MbcError):
+        F.Plan(np.array([[0.0, 0, 0], [1.0, 0, 0], [1.0, 0, 0], [0, 1.0, 0]]))
+    with pytest.raises(F.MbcError) as e:
+        F.Plan(np.array([[0.0, np.nan, 0], [1.0, 0, 0]]))
+    assert e.value.status == 4
+    with pytest.raises(F.MbcError):
+        F.Plan(np.zeros((0, 3)))
+    with pytest.raises(F.MbcError):
+        F.Plan(np.random.default_rng(0).random((10, 3)), rho=-1.0)
