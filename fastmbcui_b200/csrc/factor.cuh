@@ -32,6 +32,10 @@ struct FactorArgs {
   int32_t nf;
   double coef;
   double shift;      // relative diagonal shift (retries only)
+  // A pivot that keeps less than pivot_tol of its original diagonal entry
+  // has cancelled most of its digits: the supernode is flagged for the FP64
+  // retry (FP32 launches); 0 flags only non-positive pivots.
+  double pivot_tol;
   int32_t smem_cap;  // largest n_s kept in shared memory
   int32_t tile_rows; // panel rows per tile
   int32_t *bad_list, *bad_count;
@@ -157,13 +161,15 @@ __global__ void __launch_bounds__(NT) factor_kernel(FactorArgs a, T *__restrict_
   __syncthreads();
   if (a.shift > 0)
     for (int k = tid; k < ns; k += NT) A[k + (size_t)k * ns] += s_scal[1];
+  // keep the diagonal for the cancellation test (wbuf is free until step 3)
+  for (int k = tid; k < ns; k += NT) wbuf[k] = A[k + (size_t)k * ns];
 
   // 2. right-looking U^T U on the upper triangle
   for (int k = 0; k < ns; ++k) {
     __syncthreads();
     if (tid == 0) {
       const T d = A[k + (size_t)k * ns];
-      if (!(d > T(0))) s_bad = 1;
+      if (!(d > T(0)) || d < (T)a.pivot_tol * wbuf[k]) s_bad = 1;
       const T u = sqrt(d > T(0) ? d : T(1));
       A[k + (size_t)k * ns] = u;
       s_scal[0] = T(1) / u;

@@ -164,6 +164,9 @@ struct ClassSpec {
   int max_ns;  // inclusive upper bound of n_s for this class (0 = unbounded)
   int nt, tile_rows;
 };
+// FP32 supernodes whose pivots cancel below this fraction of their diagonal
+// (more than ~3 of FP32's ~7 digits lost) are refactored in FP64.
+constexpr double kF32PivotTol = 1e-3;
 // n_s <= 32, <= 64, <= 128 in shared memory; larger ones in global memory
 constexpr ClassSpec kClasses[4] = {{32, 128, 64}, {64, 256, 32}, {128, 512, 32}, {0, 512, 8}};
 
@@ -191,8 +194,8 @@ mbc_status launch_factor_class(FactorArgs a, T *theta, LT *lval, size_t smem, cu
 // Launch the factor kernels over the given per-class supernode lists.
 template <typename T, typename LT>
 static mbc_status run_factor(Solver &S, const std::vector<int32_t> *lists, T *theta, LT *lval,
-                             double shift, int32_t *d_bad_list, int32_t *d_bad_count,
-                             cudaStream_t st)
+                             double shift, double pivot_tol, int32_t *d_bad_list,
+                             int32_t *d_bad_count, cudaStream_t st)
 {
   const Plan &p = *S.plan;
   for (int c = 0; c < 4; ++c) {
@@ -221,6 +224,7 @@ static mbc_status run_factor(Solver &S, const std::vector<int32_t> *lists, T *th
     a.nf = S.nf;
     a.coef = S.op.coef;
     a.shift = shift;
+    a.pivot_tol = pivot_tol;
     a.bad_list = d_bad_list;
     a.bad_count = d_bad_count;
     const ClassSpec cs = kClasses[c];
@@ -283,10 +287,10 @@ mbc_status Solver::factor(cudaStream_t st)
   split_classes(p, all, lists);
   if (precision == MBC_F64)
     MBC_TRY((run_factor<double, double>(*this, lists, (double *)theta.ptr, (double *)lval.ptr, 0.0,
-                                        d_bad_list, d_bad_count, st)));
+                                        0.0, d_bad_list, d_bad_count, st)));
   else
     MBC_TRY((run_factor<float, float>(*this, lists, (float *)theta.ptr, (float *)lval.ptr, 0.0,
-                                      d_bad_list, d_bad_count, st)));
+                                      kF32PivotTol, d_bad_list, d_bad_count, st)));
   // supernodes with a non-positive pivot: redo in FP64, then FP64 with a
   // small diagonal shift
   pivot_retries = 0;
@@ -305,10 +309,10 @@ mbc_status Solver::factor(cudaStream_t st)
     MBC_TRY(theta64.reserve(std::max<size_t>(th_n * 8, 16)));
     if (precision == MBC_F64)
       MBC_TRY((run_factor<double, double>(*this, lists, (double *)theta.ptr, (double *)lval.ptr,
-                                          shifts[attempt], d_bad_list, d_bad_count, st)));
+                                          shifts[attempt], 0.0, d_bad_list, d_bad_count, st)));
     else
       MBC_TRY((run_factor<double, float>(*this, lists, (double *)theta64.ptr, (float *)lval.ptr,
-                                         shifts[attempt], d_bad_list, d_bad_count, st)));
+                                         shifts[attempt], 0.0, d_bad_list, d_bad_count, st)));
   }
   {
     int32_t nbad = 0;

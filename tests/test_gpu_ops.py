@@ -66,8 +66,11 @@ def test_vpl_matches_oracle_adjoint(setup):
     G = rng.standard_normal((sc.n, 3)).astype(np.float32)
     V = mfs.ops.VpL_fast_float(_t(K), _t(G), Vs, 3.0, 2000, 1e-6).double().cpu().numpy()
     for c in range(3):
-        # (K^T K) v = g: compare K^T K v with g
-        assert np.linalg.norm(op.KT(op.K(V[:, c])) - G[:, c]) / np.linalg.norm(G[:, c]) < 1e-3
+        xo, it, rr = O.pcg(op, pl, lval, b=G[pl["Pinv"], c].astype(np.float64), maxits=4000, tol=1e-10)
+        # K v is what the autograd formula consumes (grad_F = M VpL); the
+        # FP32-rounded v itself is ill-conditioned
+        kv, kvo = op.K(V[:, c]), op.K(xo[pl["P"]])
+        assert np.linalg.norm(kv - kvo) / np.linalg.norm(kvo) < 1e-3
 
 
 def test_autograd_formula(setup):
