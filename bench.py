@@ -26,6 +26,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+MATVEC = {"auto": 0, "simt": 1, "tensor": 2}
+
 METRIC = "MFS solves/s at rel-res 1e-8 on 1 B200: mixed+batched+learned vs plain FP64"
 
 WORKLOADS = {
@@ -153,7 +155,8 @@ def run_ours(args):
     t_plan = time.perf_counter() - t0
     x, nx, y, Fd = t(sc.x), t(sc.nx), t(sc.y), t(Fm)
     solver = F.Solver(plan, x=x, nx=nx, y=y, coef=sc.coef, precision=F.MBC_F32)
-    opts = dict(tol=1e-8, max_iters=args.max_iters, max_refine=6, inner_tol=1e-4, check_every=8)
+    solver.set_matvec(MATVEC[args.matvec])
+    opts = dict(tol=1e-8, max_iters=args.max_iters, max_refine=64, inner_tol=1e-2, check_every=8)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
 
     def step(profile=0):
@@ -191,7 +194,8 @@ def run_ours(args):
         t0 = time.perf_counter()
         dx, dnx, dy, dF = (a.to(dev, non_blocking=True) for a in (hx, hnx, hy, hF))
         pl2 = F.Plan(yh.astype(np.float64), sc.rho, sc.lam, sc.max_super)
-        s2 = F.Solver(pl2, x=dx, nx=dnx, y=dy, coef=sc.coef, precision=F.MBC_F32).factor()
+        s2 = F.Solver(pl2, x=dx, nx=dnx, y=dy, coef=sc.coef, precision=F.MBC_F32)
+        s2.set_matvec(MATVEC[args.matvec]).factor()
         X2, _ = s2.solve(dF, out_dtype=torch.float32, **opts)
         hX.copy_(X2)
         torch.cuda.synchronize()
@@ -229,7 +233,8 @@ def run_ours(args):
     achieved = flops / (launch_ms * 1e-3) / 1e12
     roofline = {"bound": "tensor", "achieved": round(achieved, 2), "peak": bf16, "unit": "TFLOP/s",
                 "frac": round(achieved / bf16, 4), "traffic": None,
-                "kernel": "pk_rows_kernel / pk_cols_kernel (FP32 SIMT, 64-column chunks)",
+                "kernel": ("pk_tc_kernel<0|1> (tcgen05 3xTF32, TMEM accumulators)" if args.matvec != "simt"
+                           else "pk_rows_kernel / pk_cols_kernel (FP32 SIMT)"),
                 "launch_ms": round(launch_ms, 3), "peak_source": f"bf16 dense, {src}",
                 "fp32_simt_nominal_tflops": 74.4}
     out = {
@@ -310,6 +315,38 @@ def cpu_baseline(sc, st, plan_gpu=None):
                        f"{iters} iterations x {R} columns")}
 
 
+def run_probe(args):
+    """A few launches of the hot kernels on the workload, for ncu captures:
+    one factor, then `--probe-reps` x (K, K^T) with all R columns (FP32)."""
+    import torch
+
+    import fastmbcui_b200 as F
+
+    build, desc = WORKLOADS[args.workload]
+    sc = build(4)
+    R = 6 * sc.n_bodies
+    dev = torch.device("cuda", 0)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
+    plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
+    solver = F.Solver(plan, x=t(sc.x), nx=t(sc.nx), y=t(sc.y), coef=sc.coef, precision=F.MBC_F32)
+    solver.set_matvec(MATVEC[args.matvec]).factor()
+    rng = np.random.default_rng(0)
+    V = t(rng.standard_normal((sc.n, R)))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    out = []
+    for _ in range(args.probe_reps):
+        ev[0].record()
+        W = solver.apply_K(V)
+        ev[1].record()
+        solver.apply_KT(W)
+        ev[2].record()
+        torch.cuda.synchronize()
+        out.append((ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])))
+    print(json.dumps({"probe": args.workload, "matvec": args.matvec, "R": R,
+                      "K_ms": [round(a, 3) for a, _ in out],
+                      "KT_ms": [round(b, 3) for _, b in out]}), flush=True)
+
+
 def run_reference(args):
     """The reference's CPU path on the host cores (the oracle port: the
     reference's own host code cannot be built here beyond the ordering)."""
@@ -357,8 +394,15 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--ref-iters", type=int, default=200)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--kernel-probe", action="store_true",
+                    help="only run a factor and a few K / K^T launches (ncu captures)")
+    ap.add_argument("--probe-reps", type=int, default=3)
+    ap.add_argument("--matvec", default="auto", choices=sorted(MATVEC),
+                    help="FP32 matvec: tensor cores (3xTF32 tcgen05) or CUDA cores")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.kernel_probe:
+        run_probe(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -11,11 +11,12 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import (MBC_F32, MBC_F64, MBC_OP_DENSE, MBC_OP_POINT_KERNEL, MBC_SCHED_BATCHED,
-                   MBC_SCHED_PER_RHS, MbcError, check, ptr)
+from ._lib import (MBC_F32, MBC_F64, MBC_MATVEC_AUTO, MBC_MATVEC_SIMT, MBC_MATVEC_TENSOR,
+                   MBC_OP_DENSE, MBC_OP_POINT_KERNEL, MBC_SCHED_BATCHED, MBC_SCHED_PER_RHS, MbcError,
+                   check, ptr)
 
 __all__ = ["Plan", "Solver", "MbcError", "load", "MBC_F32", "MBC_F64", "MBC_SCHED_BATCHED",
-           "MBC_SCHED_PER_RHS"]
+           "MBC_SCHED_PER_RHS", "MBC_MATVEC_AUTO", "MBC_MATVEC_SIMT", "MBC_MATVEC_TENSOR"]
 
 
 def load():
@@ -133,6 +134,11 @@ class Solver:
 
     def factor(self):
         check(load().mbc_solver_factor(self._h, self._sp()), "mbc_solver_factor")
+        return self
+
+    def set_matvec(self, impl: int):
+        """MBC_MATVEC_AUTO / _SIMT / _TENSOR (FP32 point-kernel solvers)."""
+        check(load().mbc_solver_set_matvec(self._h, int(impl)), "mbc_solver_set_matvec")
         return self
 
     def pivot_retries(self) -> int:

@@ -133,11 +133,11 @@ mbc_status run(mbc_context *ctx, bool adjoint, const float *M, int32_t nf, int32
   mbc_solve_default_options(&o);
   o.max_iters = (int32_t)maxit;
   o.tol = tol;
-  // One FP32 sweep (the reference's FP32 PCG, with FP64 scalars) when tol_r
-  // is within FP32 reach; below that, FP32 sweeps inside FP64 refinement so
+  // The reference's FP32 PCG (with FP64 scalars) when tol_r is within FP32
+  // reach; below that, the FP32 recursion with FP64 residual replacement so
   // the tolerance holds for the true residual.
-  o.max_refine = tol < 1e-4 ? 8 : 0;
-  o.inner_tol = 1e-4;
+  o.max_refine = tol < 1e-4 ? 64 : 0;
+  o.inner_tol = 1e-2;
   o.check_every = 4;
   mbc_solve_stats stats{};
   std::vector<int32_t> iters(R);

@@ -15,10 +15,13 @@ enum ColStatus : int32_t { COL_ACTIVE = -1, COL_OK = 0, COL_MAXIT = 1, COL_BREAK
 
 struct PcgScalars {
   double *rz, *b2, *thr, *alpha, *beta, *rr, *pt;
+  double *rr_ref;  // residual replacement: |r|^2 at the last replacement
   int32_t *status, *iters;
-  int32_t *done;  // 1 when no column is active
+  int32_t *done;   // 1 when no column is active
+  int32_t *want;   // residual replacement requested (set by RED_CHECK)
   int32_t maxit;
   double tol2;
+  double drop2;    // > 0: replacement mode, replace once |r|^2 < drop2 * rr_ref
 };
 
 // Block reduction over threadIdx.y of one double per thread; thread (x, 0)
@@ -90,11 +93,11 @@ __global__ void dot_partial_kernel(int n, int R, const T *__restrict__ a, const 
   if (threadIdx.y == 0 && c < R) part[(size_t)blockIdx.x * R + c] = s;
 }
 
-// x += alpha p; r -= alpha t; part = r . r
-template <typename T>
+// x += alpha p; r -= alpha t; part = r . r   (x may be FP64 while p, r are T)
+template <typename T, typename XT>
 __global__ void update_xr_kernel(int n, int R, const double *__restrict__ alpha,
                                  const T *__restrict__ p, const T *__restrict__ t,
-                                 T *__restrict__ x, T *__restrict__ r, double *__restrict__ part,
+                                 XT *__restrict__ x, T *__restrict__ r, double *__restrict__ part,
                                  const int32_t *__restrict__ done)
 {
   if (done && *done) return;
@@ -105,7 +108,7 @@ __global__ void update_xr_kernel(int n, int R, const double *__restrict__ alpha,
   if (c < R && i < n) {
     const size_t o = (size_t)i * R + c;
     const double a = alpha[c];
-    const T xv = (T)((double)x[o] + a * (double)p[o]);
+    const XT xv = (XT)((double)x[o] + a * (double)p[o]);
     const T rv = (T)((double)r[o] - a * (double)t[o]);
     x[o] = xv;
     r[o] = rv;
@@ -134,7 +137,8 @@ enum ReduceMode : int32_t {
   RED_INIT_B = 1,  // b2 = s, thr = tol^2 s, status ACTIVE unless |b|^2 < 1e-16
   RED_ALPHA = 2,   // alpha = rz / s (breakdown if s <= 0 or NaN)
   RED_CHECK = 3,   // rr = s, iters++, converge / max-iteration test, done flag
-  RED_BETA = 4     // beta = s / rz, rz = s
+  RED_BETA = 4,    // beta = s / rz, rz = s
+  RED_REPLACE = 5  // true |r|^2 after a residual replacement: rr = rr_ref = s, converge test
 };
 
 // One block of 1024 threads: warp per column, lanes over the partial blocks.
@@ -143,7 +147,7 @@ __global__ void __launch_bounds__(1024) reduce_kernel(int nblk, int R,
                                                       int32_t mode, PcgScalars sc,
                                                       double *__restrict__ out)
 {
-  if (mode != RED_INIT_B && mode != RED_STORE && sc.done && *sc.done) return;
+  if (mode != RED_INIT_B && mode != RED_STORE && mode != RED_REPLACE && sc.done && *sc.done) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int any = 0;
   for (int c = warp; c < R; c += 32) {
@@ -159,6 +163,7 @@ __global__ void __launch_bounds__(1024) reduce_kernel(int nblk, int R,
         case RED_INIT_B:
           sc.b2[c] = s;
           sc.thr[c] = sc.tol2 * s;
+          if (sc.rr_ref) sc.rr_ref[c] = s;
           if (sc.status[c] == COL_ACTIVE && s < 1e-16) {
             sc.status[c] = COL_OK;  // kl_chol.cu:950-953: zero right-hand side
             sc.rr[c] = 0.0;
@@ -181,9 +186,26 @@ __global__ void __launch_bounds__(1024) reduce_kernel(int nblk, int R,
           if (sc.status[c] == COL_ACTIVE) {
             sc.rr[c] = s;
             sc.iters[c] += 1;
+            if (!(s == s)) {
+              sc.status[c] = COL_BREAKDOWN;
+            } else if (sc.drop2 > 0.0) {
+              // replacement mode: convergence is only declared on a true
+              // FP64 residual, so ask for one
+              if (s < sc.thr[c] || s < sc.drop2 * sc.rr_ref[c]) *sc.want = 1;
+              if (sc.iters[c] >= sc.maxit) sc.status[c] = COL_MAXIT;
+            } else if (s < sc.thr[c]) {
+              sc.status[c] = COL_OK;
+            } else if (sc.iters[c] >= sc.maxit) {
+              sc.status[c] = COL_MAXIT;
+            }
+          }
+          break;
+        case RED_REPLACE:
+          if (sc.status[c] == COL_ACTIVE || sc.status[c] == COL_MAXIT) {
+            sc.rr[c] = s;
+            sc.rr_ref[c] = s;
             if (!(s == s)) sc.status[c] = COL_BREAKDOWN;
             else if (s < sc.thr[c]) sc.status[c] = COL_OK;
-            else if (sc.iters[c] >= sc.maxit) sc.status[c] = COL_MAXIT;
           }
           break;
         case RED_BETA:
@@ -198,7 +220,7 @@ __global__ void __launch_bounds__(1024) reduce_kernel(int nblk, int R,
       if (sc.status && sc.status[c] == COL_ACTIVE) any = 1;
     }
   }
-  if (mode == RED_CHECK || mode == RED_INIT_B || mode == RED_ALPHA) {
+  if (mode == RED_CHECK || mode == RED_INIT_B || mode == RED_ALPHA || mode == RED_REPLACE) {
     any = __syncthreads_or(any);
     if (threadIdx.x == 0 && sc.done) *sc.done = any ? 0 : 1;
   }

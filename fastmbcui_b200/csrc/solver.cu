@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -13,6 +14,7 @@
 
 #include "factor.cuh"
 #include "matvec.cuh"
+#include "matvec_tc.cuh"
 #include "mbc_internal.h"
 #include "pcg.cuh"
 #include "solver.h"
@@ -76,27 +78,47 @@ static mbc_status upload(DevMem &m, const std::vector<V> &h, cudaStream_t st)
 // --------------------------------------------------------------------------
 namespace {
 
-constexpr int TI_ROWS = 128, TJ_ROWS = 128;
-constexpr int TI_COLS = 128, TJ_COLS = 64;
+constexpr int TJ_ROWS = 128;
+constexpr int TJ_COLS = 64;
+
+// Launch shape for a direction with `rows` outputs and R columns: the widest
+// column chunk RC (fewest kernel re-evaluations) and the larger block TI that
+// still give at least four blocks per SM; otherwise the shape with the most
+// blocks.
+struct Shape {
+  int ti, rc;
+};
 
 template <typename T>
-int pick_rc(int R)
+Shape pick_shape(int rows, int R)
 {
-  if (R == 1) return 1;
-  if (R <= 4) return 4;
-  if (R <= 8) return 8;
-  if (R <= 16) return 16;
-  if (sizeof(T) == 8) return 32;
-  return R <= 32 ? 32 : 64;
+  const int want = 4 * 148;
+  if (R == 1) return {rows >= 128 * want ? 128 : 64, 1};
+  static const Shape f32[] = {{128, 64}, {128, 32}, {64, 32}, {64, 16}, {64, 8}, {64, 4}};
+  static const Shape f64[] = {{128, 32}, {64, 32}, {64, 16}, {64, 8}, {64, 4}};
+  const Shape *c = sizeof(T) == 8 ? f64 : f32;
+  const int nc = sizeof(T) == 8 ? 5 : 6;
+  Shape best = c[0];
+  int64_t best_blocks = -1;
+  for (int k = 0; k < nc; ++k) {
+    if (c[k].rc > 4 && c[k].rc / 2 >= R) continue;  // chunk much wider than R
+    const int64_t blocks = (int64_t)cdiv(rows, c[k].ti) * cdiv(R, c[k].rc);
+    if (blocks >= want) return c[k];
+    if (blocks > best_blocks) {
+      best = c[k];
+      best_blocks = blocks;
+    }
+  }
+  return best;
 }
 
-template <typename T, int RC>
+template <typename T, int RC, int TI>
 void rows_launch(const Solver &S, int R, const T *v, T *w, const int32_t *done, cudaStream_t st)
 {
   if (S.op.kind == MBC_OP_POINT_KERNEL) {
-    dim3 grid(cdiv(S.nf, TI_ROWS), cdiv(R, RC));
-    pk_rows_kernel<T, RC, TI_ROWS, TJ_ROWS><<<grid, TI_ROWS, 0, st>>>(
-        S.x4(), S.n4(), S.nf, S.y4(), S.n, v, R, (T)S.op.coef, w, R, R, done);
+    dim3 grid(cdiv(S.nf, TI), cdiv(R, RC));
+    pk_rows_kernel<T, RC, TI, TJ_ROWS><<<grid, TI, 0, st>>>(S.x4(), S.n4(), S.nf, S.y4(), S.n, v, R,
+                                                            (T)S.op.coef, w, R, R, done);
   } else {
     dim3 grid(cdiv(S.nf, 8), cdiv(R, RC));
     dense_rows_kernel<T, RC><<<grid, 256, 0, st>>>(S.op.M, S.op.ldm, S.nf, S.n, S.dP(), v, R, w,
@@ -104,51 +126,102 @@ void rows_launch(const Solver &S, int R, const T *v, T *w, const int32_t *done, 
   }
 }
 
-template <typename T, int RC>
+template <typename T, int RC, int TI>
 int cols_launch(const Solver &S, int R, const T *w, T *t, const T *pdot, double *part,
                 const int32_t *done, cudaStream_t st)
 {
-  dim3 grid(cdiv(S.n, TI_COLS), cdiv(R, RC));
+  dim3 grid(cdiv(S.n, TI), cdiv(R, RC));
   if (S.op.kind == MBC_OP_POINT_KERNEL) {
-    pk_cols_kernel<T, RC, TI_COLS, TJ_COLS><<<grid, TI_COLS, 0, st>>>(
-        S.x4(), S.n4(), S.nf, S.y4(), S.n, w, R, (T)S.op.coef, t, R, R, pdot, part, done);
+    pk_cols_kernel<T, RC, TI, TJ_COLS><<<grid, TI, 0, st>>>(S.x4(), S.n4(), S.nf, S.y4(), S.n, w, R,
+                                                            (T)S.op.coef, t, R, R, pdot, part, done);
   } else {
-    dense_cols_kernel<T, RC, TI_COLS, 32><<<grid, TI_COLS, 0, st>>>(
-        S.op.M, S.op.ldm, S.nf, S.n, S.dP(), w, R, t, R, R, pdot, part, done);
+    dense_cols_kernel<T, RC, TI, 32><<<grid, TI, 0, st>>>(S.op.M, S.op.ldm, S.nf, S.n, S.dP(), w, R,
+                                                          t, R, R, pdot, part, done);
   }
   return (int)grid.x;
 }
 
 }  // namespace
 
+// tensor-core path: FP32 point kernel, 8 <= R <= 256
+static bool use_tc(const Solver &S, int R)
+{
+  if (S.op.kind != MBC_OP_POINT_KERNEL || R > 256) return false;
+  if (S.matvec_impl == MBC_MATVEC_SIMT) return false;
+  if (S.matvec_impl == MBC_MATVEC_TENSOR) return true;
+  return R >= 8;
+}
+
+template <int DIR>
+static int tc_launch(const Solver &S, int R, const float *vin, float *out, const float *pdot,
+                     double *part, const int32_t *done, cudaStream_t st)
+{
+  tc::TcArgs a{};
+  a.xr = S.x4();
+  a.nr = S.n4();
+  a.ys = S.y4();
+  a.nf = S.nf;
+  a.n = S.n;
+  a.vin = vin;
+  a.out = out;
+  a.R = R;
+  a.np = (R + 15) / 16 * 16;
+  a.tmem_cols = a.np <= 32 ? 32 : a.np <= 64 ? 64 : a.np <= 128 ? 128 : 256;
+  a.coef = (float)S.op.coef;
+  a.pdot = pdot;
+  a.part = part;
+  a.done = done;
+  a.err = (int32_t *)S.m_err.ptr;
+  cudaFuncSetAttribute(tc::pk_tc_kernel<DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       tc::smem_bytes(256));
+  const int M = DIR == 0 ? S.nf : S.n;
+  const unsigned grid = cdiv(M, tc::kM);
+  tc::pk_tc_kernel<DIR><<<grid, tc::kThreads, tc::smem_bytes(a.np), st>>>(a);
+  return (int)grid;
+}
+
+#define MBC_SHAPES(T, X)                                                   \
+  X(T, 1, 64) X(T, 1, 128) X(T, 4, 64) X(T, 8, 64) X(T, 16, 64) X(T, 32, 64) X(T, 32, 128)
+
 template <typename T>
 void launch_rows(const Solver &S, int R, const T *v, T *w, const int32_t *done, cudaStream_t st)
 {
-  switch (pick_rc<T>(R)) {
-    case 1: rows_launch<T, 1>(S, R, v, w, done, st); break;
-    case 4: rows_launch<T, 4>(S, R, v, w, done, st); break;
-    case 8: rows_launch<T, 8>(S, R, v, w, done, st); break;
-    case 16: rows_launch<T, 16>(S, R, v, w, done, st); break;
-    case 32: rows_launch<T, 32>(S, R, v, w, done, st); break;
-    default: rows_launch<T, (sizeof(T) == 8 ? 32 : 64)>(S, R, v, w, done, st); break;
+  if constexpr (sizeof(T) == 4) {
+    if (use_tc(S, R)) {
+      tc_launch<0>(S, R, v, w, nullptr, nullptr, done, st);
+      return;
+    }
   }
+  const Shape sh = pick_shape<T>(S.op.kind == MBC_OP_POINT_KERNEL ? S.nf : 1 << 30, R);
+#define MBC_ROWS_CASE(TT, RC_, TI_) \
+  if (sh.rc == RC_ && sh.ti == TI_) return rows_launch<T, RC_, TI_>(S, R, v, w, done, st);
+  MBC_SHAPES(T, MBC_ROWS_CASE)
+  if constexpr (sizeof(T) == 4) {
+    if (sh.rc == 64) return rows_launch<T, 64, 128>(S, R, v, w, done, st);
+  }
+#undef MBC_ROWS_CASE
+  rows_launch<T, 32, 64>(S, R, v, w, done, st);
 }
 
 template <typename T>
 int launch_cols(const Solver &S, int R, const T *w, T *t, const T *pdot, double *part,
                 const int32_t *done, cudaStream_t st)
 {
-  switch (pick_rc<T>(R)) {
-    case 1: return cols_launch<T, 1>(S, R, w, t, pdot, part, done, st);
-    case 4: return cols_launch<T, 4>(S, R, w, t, pdot, part, done, st);
-    case 8: return cols_launch<T, 8>(S, R, w, t, pdot, part, done, st);
-    case 16: return cols_launch<T, 16>(S, R, w, t, pdot, part, done, st);
-    case 32: return cols_launch<T, 32>(S, R, w, t, pdot, part, done, st);
-    default: return cols_launch<T, (sizeof(T) == 8 ? 32 : 64)>(S, R, w, t, pdot, part, done, st);
+  if constexpr (sizeof(T) == 4) {
+    if (use_tc(S, R)) return tc_launch<1>(S, R, w, t, pdot, part, done, st);
   }
+  const Shape sh = pick_shape<T>(S.n, R);
+#define MBC_COLS_CASE(TT, RC_, TI_) \
+  if (sh.rc == RC_ && sh.ti == TI_) return cols_launch<T, RC_, TI_>(S, R, w, t, pdot, part, done, st);
+  MBC_SHAPES(T, MBC_COLS_CASE)
+  if constexpr (sizeof(T) == 4) {
+    if (sh.rc == 64) return cols_launch<T, 64, 128>(S, R, w, t, pdot, part, done, st);
+  }
+#undef MBC_COLS_CASE
+  return cols_launch<T, 32, 64>(S, R, w, t, pdot, part, done, st);
 }
 
-int cols_blocks(const Solver &S) { return (int)cdiv(S.n, TI_COLS); }
+int cols_blocks(const Solver &S) { return (int)cdiv(S.n, 64); }
 
 template void launch_rows<float>(const Solver &, int, const float *, float *, const int32_t *, cudaStream_t);
 template void launch_rows<double>(const Solver &, int, const double *, double *, const int32_t *, cudaStream_t);
@@ -351,6 +424,8 @@ mbc_status Solver::create(const Plan &pl, const mbc_operator &o, int32_t prec, c
   MBC_TRY(upload(m_rcol, pl.rcol, st));
   MBC_TRY(upload(m_rmap, pl.rmap, st));
   MBC_TRY(upload(m_th_ptr, pl.th_ptr, st));
+  MBC_TRY(m_err.reserve(sizeof(int32_t)));
+  MBC_CK(cudaMemsetAsync(m_err.ptr, 0, sizeof(int32_t), st));
   if (o.kind == MBC_OP_POINT_KERNEL) {
     MBC_TRY(m_x4.reserve(sizeof(float4) * nf));
     MBC_TRY(m_n4.reserve(sizeof(float4) * nf));
@@ -389,10 +464,12 @@ Layout2D layout2d(int n, int R)
 
 }  // namespace
 
-// Work buffers for one precision.
+// Work buffers for one precision.  X64 is the FP64 solution accumulator of
+// the residual-replacement mode.
 template <typename T>
 struct PcgWork {
   T *X, *Rv, *Pv, *Z, *U, *Tt, *W;
+  double *X64 = nullptr;
   double *part;
   int part_stride;  // blocks
   PcgScalars sc;
@@ -418,7 +495,7 @@ static mbc_status pcg_buffers(Solver &S, int R, PcgWork<T> &w)
   w.part_stride = nblk;
   MBC_TRY(S.part.reserve(sizeof(double) * (size_t)nblk * R));
   w.part = (double *)S.part.ptr;
-  MBC_TRY(S.scal.reserve(sizeof(double) * 7 * R + sizeof(int32_t) * (2 * R + 4)));
+  MBC_TRY(S.scal.reserve(sizeof(double) * 8 * R + sizeof(int32_t) * (2 * R + 4)));
   double *d = (double *)S.scal.ptr;
   w.sc.rz = d;
   w.sc.b2 = d + R;
@@ -427,21 +504,28 @@ static mbc_status pcg_buffers(Solver &S, int R, PcgWork<T> &w)
   w.sc.beta = d + 4 * R;
   w.sc.rr = d + 5 * R;
   w.sc.pt = d + 6 * R;
-  int32_t *ii = (int32_t *)(d + 7 * R);
+  w.sc.rr_ref = d + 7 * R;
+  int32_t *ii = (int32_t *)(d + 8 * R);
   w.sc.status = ii;
   w.sc.iters = ii + R;
   w.sc.done = ii + 2 * R;
+  w.sc.want = ii + 2 * R + 1;
+  w.sc.drop2 = 0.0;
   return MBC_OK;
 }
 
 __global__ void set_status_kernel(int R, int32_t *status, int32_t *iters, int32_t *done,
-                                  const int32_t *mask)
+                                  int32_t *want, double *rz, const int32_t *mask)
 {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c == 0) *done = 0;
+  if (c == 0) {
+    *done = 0;
+    *want = 0;
+  }
   if (c >= R) return;
   status[c] = (mask == nullptr || mask[c]) ? COL_ACTIVE : COL_OK;
   iters[c] = 0;
+  rz[c] = __longlong_as_double(0x7ff0000000000000LL);  // +inf: the first beta is 0
 }
 
 // Warm starts: thresholds relative to |b|^2 of the original right-hand side.
@@ -454,75 +538,85 @@ __global__ void set_thresholds_kernel(int R, double tol2, const double *b2ref, P
   if (b2ref[c] < 1e-16 && sc.status[c] == COL_ACTIVE) sc.status[c] = COL_OK;
 }
 
-// Run PCG on (K^T K) x = b for R columns.  On entry w.Rv holds b (new order)
-// and w.X the starting point whose residual b - K^T K x is already in w.Rv.
-// Columns with mask[c] == 0 are skipped.  Returns after every column stopped.
-template <typename T, typename LT>
-static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, const LT *lval, int maxit, double tol,
-                          bool precond, int check_every, const int32_t *d_mask, cudaStream_t st,
-                          const double *d_b2ref = nullptr)
+// Run PCG on (K^T K) x = b for R columns (the recurrences of kl_chol.cu:975-1078
+// per column).  On entry w.Rv holds the residual b - K^T K x of the start x
+// (x = w.X, or w.X64 when `replace` is given).  One iteration here is
+//   z = L L^T r, beta = r.z / rz_old, p = z + beta p, t = K^T K p,
+//   alpha = r.z / p.t, x += alpha p, r -= alpha t, stop test on |r|^2,
+// so a host check point falls right after the residual update: that is
+// where `replace` (residual replacement) swaps in the FP64 true residual,
+// keeping p and therefore the Krylov information.
+template <typename T, typename LT, typename XT>
+static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, XT *x, const LT *lval, int maxit,
+                          double tol, bool precond, int check_every, const int32_t *d_mask,
+                          cudaStream_t st, const double *d_b2ref,
+                          const std::function<mbc_status()> *replace, int max_replace)
 {
-  const Plan &p = *S.plan;
   const Layout2D L = layout2d(S.n, R);
   const int nblk2 = (int)L.grid.x;
   w.sc.maxit = maxit;
   w.sc.tol2 = tol * tol;
-  set_status_kernel<<<cdiv(R, 256), 256, 0, st>>>(R, w.sc.status, w.sc.iters, w.sc.done, d_mask);
+  set_status_kernel<<<cdiv(R, 256), 256, 0, st>>>(R, w.sc.status, w.sc.iters, w.sc.done, w.sc.want,
+                                                   w.sc.rz, d_mask);
   // |b|^2 and the stopping thresholds
   dot_partial_kernel<T><<<L.grid, L.block, L.smem, st>>>(S.n, R, w.Rv, w.Rv, w.part);
   reduce_kernel<<<1, 1024, 0, st>>>(nblk2, R, w.part, RED_INIT_B, w.sc, nullptr);
   if (d_b2ref) set_thresholds_kernel<<<cdiv(R, 256), 256, 0, st>>>(R, w.sc.tol2, d_b2ref, w.sc);
-  // z = L L^T r, rz = r.z, p = z
-  auto apply_precond = [&](const T *r, T *z) {
-    if (precond) {
-      precond_lt_kernel<T, LT><<<L.grid, L.block, 0, st>>>(S.n, R, S.d_lptr(), S.d_lind(), lval, r,
-                                                            w.U, w.sc.done);
-      precond_l_kernel<T, LT><<<L.grid, L.block, L.smem, st>>>(S.n, R, S.d_rptr(), S.d_rcol(),
-                                                               S.d_rmap(), lval, w.U, z, r, w.part,
-                                                               w.sc.done);
-    } else {
-      cudaMemcpyAsync(z, r, sizeof(T) * (size_t)S.n * R, cudaMemcpyDeviceToDevice, st);
-      dot_partial_kernel<T><<<L.grid, L.block, L.smem, st>>>(S.n, R, r, z, w.part);
-    }
-  };
-  apply_precond(w.Rv, w.Pv);
-  reduce_kernel<<<1, 1024, 0, st>>>(nblk2, R, w.part, RED_STORE, w.sc, w.sc.rz);
+  MBC_CK(cudaMemsetAsync(w.Pv, 0, sizeof(T) * (size_t)S.n * R, st));
   MBC_CKL();
-  (void)p;
-  S.launches += (d_b2ref ? 4 : 3) + 3;
-  int32_t *h_done = S.h_flag;
+  S.launches += (d_b2ref ? 4 : 3);
+  int32_t *h_flags = S.h_flag;  // [done, want]
   if (S.profile) MBC_TRY(S.ensure_events(2 * check_every));
+  int replaced = 0;
   for (int it = 0; it < maxit; it += check_every) {
     const int kmax = std::min(check_every, maxit - it);
     for (int k = 0; k < kmax; ++k) {
+      if (precond) {
+        precond_lt_kernel<T, LT><<<L.grid, L.block, 0, st>>>(S.n, R, S.d_lptr(), S.d_lind(), lval,
+                                                              w.Rv, w.U, w.sc.done);
+        precond_l_kernel<T, LT><<<L.grid, L.block, L.smem, st>>>(S.n, R, S.d_rptr(), S.d_rcol(),
+                                                                 S.d_rmap(), lval, w.U, w.Z, w.Rv,
+                                                                 w.part, w.sc.done);
+      } else {
+        MBC_CK(cudaMemcpyAsync(w.Z, w.Rv, sizeof(T) * (size_t)S.n * R, cudaMemcpyDeviceToDevice, st));
+        dot_partial_kernel<T><<<L.grid, L.block, L.smem, st>>>(S.n, R, w.Rv, w.Z, w.part);
+      }
+      reduce_kernel<<<1, 1024, 0, st>>>(nblk2, R, w.part, RED_BETA, w.sc, nullptr);
+      update_p_kernel<T><<<L.grid, L.block, 0, st>>>(S.n, R, w.sc.beta, w.sc.status, w.Z, w.Pv,
+                                                      w.sc.done);
       if (S.profile) MBC_CK(cudaEventRecord(S.events[2 * k], st));
       launch_rows<T>(S, R, w.Pv, w.W, w.sc.done, st);
       const int nb = launch_cols<T>(S, R, w.W, w.Tt, w.Pv, w.part, w.sc.done, st);
       if (S.profile) MBC_CK(cudaEventRecord(S.events[2 * k + 1], st));
       reduce_kernel<<<1, 1024, 0, st>>>(nb, R, w.part, RED_ALPHA, w.sc, nullptr);
-      update_xr_kernel<T><<<L.grid, L.block, L.smem, st>>>(S.n, R, w.sc.alpha, w.Pv, w.Tt, w.X,
-                                                           w.Rv, w.part, w.sc.done);
+      update_xr_kernel<T, XT><<<L.grid, L.block, L.smem, st>>>(S.n, R, w.sc.alpha, w.Pv, w.Tt, x,
+                                                               w.Rv, w.part, w.sc.done);
       reduce_kernel<<<1, 1024, 0, st>>>(nblk2, R, w.part, RED_CHECK, w.sc, nullptr);
-      apply_precond(w.Rv, w.Z);
-      reduce_kernel<<<1, 1024, 0, st>>>(nblk2, R, w.part, RED_BETA, w.sc, nullptr);
-      update_p_kernel<T><<<L.grid, L.block, 0, st>>>(S.n, R, w.sc.beta, w.sc.status, w.Z, w.Pv,
-                                                      w.sc.done);
-      S.launches += 9;
+      S.launches += precond ? 9 : 8;
     }
     MBC_CKL();
-    MBC_CK(cudaMemcpyAsync(h_done, w.sc.done, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    MBC_CK(cudaMemcpyAsync(h_flags, w.sc.done, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     MBC_CK(cudaStreamSynchronize(st));
     if (S.profile) {
-      // only iterations that still had an active column did real work; the
-      // done flag is read at the start of each matvec kernel
+      // iterations after the last active column stopped exit at once; they
+      // are filtered out when the stats are formed
       for (int k = 0; k < kmax; ++k) {
         float ms = 0.f;
         MBC_CK(cudaEventElapsedTime(&ms, S.events[2 * k], S.events[2 * k + 1]));
         S.prof_ms_all.push_back(ms);
       }
     }
-    if (*h_done) break;
+    if (h_flags[0]) break;
+    if (replace && h_flags[1] && replaced < max_replace) {
+      MBC_TRY((*replace)());
+      ++replaced;
+      MBC_CK(cudaMemsetAsync(w.sc.want, 0, sizeof(int32_t), st));
+      MBC_CK(cudaMemcpyAsync(h_flags, w.sc.done, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      MBC_CK(cudaStreamSynchronize(st));
+      if (h_flags[0]) break;
+    }
   }
+  S.replacements = replaced;
   return MBC_OK;
 }
 
@@ -692,11 +786,13 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
     b2 = (const double *)b2ref.ptr;
   }
   if (precision == MBC_F64)
-    MBC_TRY((run_pcg<T, double>(*this, R, w, (const double *)lval.ptr, o.max_iters, o.tol,
-                                o.precondition != 0, std::max(1, o.check_every), nullptr, st, b2)));
+    MBC_TRY((run_pcg<T, double, T>(*this, R, w, w.X, (const double *)lval.ptr, o.max_iters, o.tol,
+                                   o.precondition != 0, std::max(1, o.check_every), nullptr, st, b2,
+                                   nullptr, 0)));
   else
-    MBC_TRY((run_pcg<T, float>(*this, R, w, (const float *)lval.ptr, o.max_iters, o.tol,
-                               o.precondition != 0, std::max(1, o.check_every), nullptr, st, b2)));
+    MBC_TRY((run_pcg<T, float, T>(*this, R, w, w.X, (const float *)lval.ptr, o.max_iters, o.tol,
+                                  o.precondition != 0, std::max(1, o.check_every), nullptr, st, b2,
+                                  nullptr, 0)));
   std::vector<int32_t> status, iters;
   std::vector<double> rel;
   MBC_TRY(collect<T>(*this, R, w, status, iters, rel, st));
@@ -735,8 +831,14 @@ mbc_status Solver::true_residual(int R, const void *F, int32_t f_dt, const void 
   return MBC_OK;
 }
 
-// Mixed precision: FP32 PCG sweeps inside an FP64 iterative-refinement loop
-// on the true residual r = K^T (f - K x).
+// Mixed precision: one FP32 PCG recursion (FP32 matvec, factor and
+// preconditioner; FP64 scalars and dot products) with the solution
+// accumulated in FP64 and residual replacement: whenever a column's
+// recursive |r|^2 has dropped by inner_tol^2 since the last replacement, or
+// reaches the threshold, r is replaced by the FP64 true residual
+// K^T (f - K x) (b - K^T K x for the adjoint).  A column converges only on a
+// true residual, so tol is met in FP64 terms; the search direction survives
+// each replacement, so the Krylov information is not thrown away.
 mbc_status Solver::solve_mixed(int R, const void *rhs, int32_t rhs_dt, void *X, int32_t x_dt,
                                const void *X0, bool adjoint, const mbc_solve_options &o,
                                mbc_solve_stats *stats, int32_t *iters_host, cudaStream_t st)
@@ -753,69 +855,62 @@ mbc_status Solver::solve_mixed(int R, const void *rhs, int32_t rhs_dt, void *X, 
   else {
     load_rows<double>(*this, R, rhs, rhs_dt, Fd, st);
     launch_cols<double>(*this, R, Fd, Bd, nullptr, nullptr, nullptr, st);
+    ++launches;
   }
   if (X0) permute_in<double>(*this, R, X0, x_dt, Xd, st);
   else MBC_CK(cudaMemsetAsync(Xd, 0, sizeof(double) * nv, st));
   MBC_CKL();
-  std::vector<double> nb;
-  MBC_TRY(col_norms2<double>(*this, R, Bd, nb, st));
   PcgWork<float> w;
   MBC_TRY(pcg_buffers<float>(*this, R, w));
-  MBC_TRY(mask.reserve(sizeof(int32_t) * R));
-  std::vector<int32_t> hmask(R), it_total(R, 0), status(R, COL_MAXIT);
-  std::vector<double> rel(R, 1.0);
-  int sweeps = 0;
-  const int max_refine = std::max(1, o.max_refine);
-  bool have_x = X0 != nullptr;
-  for (int sweep = 0; sweep <= max_refine; ++sweep) {
-    // true residual
-    if (have_x) {
-      if (adjoint) {
-        launch_rows<double>(*this, R, Xd, Wd, nullptr, st);
-        launch_cols<double>(*this, R, Wd, Rd, nullptr, nullptr, nullptr, st);
-        sub_kernel<double><<<cdiv(nv, 256), 256, 0, st>>>(nv, Bd, Rd, Rd);
-      } else {
-        residual<double>(*this, R, Fd, Xd, Wd, Rd, st);
-      }
+  const Layout2D L = layout2d(n, R);
+  // r64 = b - K^T K x64 (FP64), r = (float) r64
+  auto true_residual_into_r = [&]() -> mbc_status {
+    if (adjoint) {
+      launch_rows<double>(*this, R, Xd, Wd, nullptr, st);
+      launch_cols<double>(*this, R, Wd, Rd, nullptr, nullptr, nullptr, st);
+      sub_kernel<double><<<cdiv(nv, 256), 256, 0, st>>>(nv, Bd, Rd, Rd);
+      launches += 3;
     } else {
-      MBC_CK(cudaMemcpyAsync(Rd, Bd, sizeof(double) * nv, cudaMemcpyDeviceToDevice, st));
+      residual<double>(*this, R, Fd, Xd, Wd, Rd, st);
     }
-    std::vector<double> nr;
-    MBC_TRY(col_norms2<double>(*this, R, Rd, nr, st));
-    bool all = true;
-    for (int c = 0; c < R; ++c) {
-      rel[c] = nb[c] < 1e-16 ? 0.0 : std::sqrt(nr[c] / nb[c]);
-      hmask[c] = rel[c] > o.tol;
-      if (hmask[c]) all = false;
-      else status[c] = COL_OK;
-    }
-    if (all || sweep == max_refine) break;
-    // inner FP32 PCG on (K^T K) d = r, relative tolerance inner_tol
-    MBC_CK(cudaMemcpyAsync(mask.ptr, hmask.data(), sizeof(int32_t) * R, cudaMemcpyHostToDevice, st));
     convert<double, float>((int64_t)nv, Rd, w.Rv, st);
-    MBC_CK(cudaMemsetAsync(w.X, 0, sizeof(float) * nv, st));
-    MBC_TRY((run_pcg<float, float>(*this, R, w, (const float *)lval.ptr, o.max_iters,
-                                   std::max(o.inner_tol, 1e-7), o.precondition != 0,
-                                   std::max(1, o.check_every), (const int32_t *)mask.ptr, st)));
-    std::vector<int32_t> st_in, it_in;
-    std::vector<double> rel_in;
-    MBC_TRY(collect<float>(*this, R, w, st_in, it_in, rel_in, st));
-    for (int c = 0; c < R; ++c) {
-      it_total[c] += it_in[c];
-      if (st_in[c] == COL_BREAKDOWN) status[c] = COL_BREAKDOWN;
-    }
-    accumulate_kernel<float><<<cdiv(nv, 256), 256, 0, st>>>(n, R, w.X, Xd);
+    ++launches;
     MBC_CKL();
-    have_x = true;
-    ++sweeps;
+    return MBC_OK;
+  };
+  if (X0) MBC_TRY(true_residual_into_r());
+  else {
+    convert<double, float>((int64_t)nv, Bd, w.Rv, st);
+    ++launches;
   }
+  // thresholds relative to |b|^2 in FP64
+  MBC_TRY(b2ref.reserve(sizeof(double) * R));
+  MBC_TRY(col_norms2_dev<double>(*this, R, Bd, (double *)b2ref.ptr, st));
+  std::function<mbc_status()> replace = [&]() -> mbc_status {
+    MBC_TRY(true_residual_into_r());
+    dot_partial_kernel<double><<<L.grid, L.block, L.smem, st>>>(n, R, Rd, Rd, w.part);
+    reduce_kernel<<<1, 1024, 0, st>>>((int)L.grid.x, R, w.part, RED_REPLACE, w.sc, nullptr);
+    launches += 2;
+    MBC_CKL();
+    return MBC_OK;
+  };
+  const double drop = std::min(std::max(o.inner_tol, 1e-6), 0.5);
+  w.sc.drop2 = drop * drop;
+  const int max_replace = o.max_refine > 0 ? std::max(o.max_refine, 1) : 0;
+  MBC_TRY((run_pcg<float, float, double>(*this, R, w, Xd, (const float *)lval.ptr, o.max_iters, o.tol,
+                                         o.precondition != 0, std::max(1, o.check_every), nullptr, st,
+                                         (const double *)b2ref.ptr, &replace, max_replace)));
+  // final true residual for every column (the status of columns that hit
+  // max_iters is re-judged on it)
+  MBC_TRY(replace());
+  std::vector<int32_t> status, iters;
+  std::vector<double> rel;
+  MBC_TRY(collect<float>(*this, R, w, status, iters, rel, st));
   permute_out<double>(*this, R, Xd, X, x_dt, st);
   MBC_CKL();
-  for (int c = 0; c < R; ++c)
-    if (status[c] != COL_OK && status[c] != COL_BREAKDOWN) status[c] = COL_MAXIT;
-  MBC_TRY(finish_stats(R, status, it_total, rel, stats, iters_host));
+  MBC_TRY(finish_stats(R, status, iters, rel, stats, iters_host));
   if (stats) {
-    stats->refinements = sweeps;
+    stats->refinements = replacements + 1;
     double m = 0;
     for (int c = 0; c < R; ++c) m = std::max(m, rel[c]);
     stats->true_relres_max = m;
@@ -907,6 +1002,7 @@ mbc_status Solver::solve(int R, const void *rhs, int32_t rhs_dt, void *X, int32_
         }
     }
   }
+  MBC_TRY(check_device_error(st));
   if (stats && stats->status_per_worst == 2) return fail(MBC_BREAKDOWN, "PCG breakdown (p.Ap <= 0 or NaN)");
   if (stats && stats->status_per_worst == 1) return fail(MBC_NOT_CONVERGED, "PCG reached max_iters above tol");
   return MBC_OK;
@@ -961,6 +1057,18 @@ mbc::Solver::~Solver()
   for (cudaEvent_t e : events) cudaEventDestroy(e);
 }
 
+mbc_status mbc::Solver::check_device_error(cudaStream_t st)
+{
+  int32_t e = 0;
+  MBC_CK(cudaMemcpyAsync(&e, m_err.ptr, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  MBC_CK(cudaStreamSynchronize(st));
+  if (e) {
+    MBC_CK(cudaMemsetAsync(m_err.ptr, 0, sizeof(int32_t), st));
+    return fail(MBC_TIMEOUT, "a bounded device wait expired in the tensor-core matvec");
+  }
+  return MBC_OK;
+}
+
 mbc_status mbc::Solver::ensure_events(int count)
 {
   while ((int)events.size() < count) {
@@ -1012,6 +1120,14 @@ extern "C" mbc_status mbc_solver_get_pivot_retries(const mbc_solver *s, int32_t 
   return MBC_OK;
 }
 
+extern "C" mbc_status mbc_solver_set_matvec(mbc_solver *s, int32_t impl)
+{
+  if (!s) return fail(MBC_BAD_ARG, "NULL solver");
+  if (impl < MBC_MATVEC_AUTO || impl > MBC_MATVEC_TENSOR) return fail(MBC_BAD_ARG, "unknown matvec implementation");
+  s->s.matvec_impl = impl;
+  return MBC_OK;
+}
+
 extern "C" void mbc_solve_default_options(mbc_solve_options *o)
 {
   if (!o) return;
@@ -1019,8 +1135,8 @@ extern "C" void mbc_solve_default_options(mbc_solve_options *o)
   o->tol = 1e-8;
   o->schedule = MBC_SCHED_BATCHED;
   o->precondition = 1;
-  o->max_refine = 4;
-  o->inner_tol = 1e-4;
+  o->max_refine = 64;
+  o->inner_tol = 1e-2;
   o->check_every = 8;
   o->true_residual = 0;
 }
@@ -1074,8 +1190,7 @@ extern "C" mbc_status mbc_apply_K(mbc_solver *s, int32_t R, const void *V, void 
     mbc::launch_rows<float>(S, R, (const float *)S.tmp.ptr, (float *)W, nullptr, st);
   }
   MBC_CKL();
-  MBC_CK(cudaStreamSynchronize(st));
-  return MBC_OK;
+  return S.check_device_error(st);
 }
 
 extern "C" mbc_status mbc_apply_KT(mbc_solver *s, int32_t R, const void *W, void *T, mbc_stream stream)
@@ -1093,6 +1208,5 @@ extern "C" mbc_status mbc_apply_KT(mbc_solver *s, int32_t R, const void *W, void
     mbc::permute_out<float>(S, R, (const float *)S.tmp.ptr, T, MBC_F32, st);
   }
   MBC_CKL();
-  MBC_CK(cudaStreamSynchronize(st));
-  return MBC_OK;
+  return S.check_device_error(st);
 }

@@ -30,7 +30,9 @@ struct Solver {
   int32_t pivot_retries = 0;
   int32_t *h_flag = nullptr;  // pinned
   int64_t launches = 0;       // kernels launched by this solver (solve paths)
+  int32_t replacements = 0;   // residual replacements in the last PCG run
   bool profile = false;
+  int32_t matvec_impl = MBC_MATVEC_AUTO;
   std::vector<cudaEvent_t> events;
   std::vector<float> prof_ms_all;
 
@@ -40,6 +42,7 @@ struct Solver {
   DevMem class_list[4];
   // operator: rows (original order) and sources (new order) as float4
   DevMem m_x4, m_n4, m_y4;
+  DevMem m_err;  // set by a tensor-core kernel whose bounded wait expired
   // factor
   DevMem theta, theta64, lval, bad, fscratch;
   // PCG workspaces
@@ -65,6 +68,7 @@ struct Solver {
 
   mbc_status create(const Plan &pl, const mbc_operator &o, int32_t prec, cudaStream_t st);
   mbc_status ensure_events(int count);
+  mbc_status check_device_error(cudaStream_t st);
   mbc_status factor(cudaStream_t st);
   mbc_status solve(int R, const void *rhs, int32_t rhs_dt, void *X, int32_t x_dt, const void *X0,
                    bool adjoint, const mbc_solve_options &o, mbc_solve_stats *stats,

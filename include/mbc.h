@@ -129,8 +129,19 @@ mbc_status mbc_solver_factor(mbc_solver *s, mbc_stream stream);
  * theta[theta_nnz] (per supernode, reversed, column-major, U in the upper part;
  * NULL to skip).  Values are widened to double. */
 mbc_status mbc_solver_get_factor(const mbc_solver *s, double *lval_host, double *theta_host);
-/* Number of supernodes whose Cholesky needed the FP64 diagonal-shift retry. */
+/* Number of supernodes refactored in FP64 (FP32 solvers: cancelling or
+ * non-positive pivots; FP64 solvers: the diagonal-shift retry). */
 mbc_status mbc_solver_get_pivot_retries(const mbc_solver *s, int32_t *count);
+
+typedef enum {
+  MBC_MATVEC_AUTO = 0,   /* tensor cores for FP32 point-kernel matvecs with 8 <= R <= 256 */
+  MBC_MATVEC_SIMT = 1,   /* CUDA-core kernels only */
+  MBC_MATVEC_TENSOR = 2  /* tensor cores whenever R <= 256 (FP32 point kernel) */
+} mbc_matvec_impl;
+
+/* Choose the matvec implementation of an FP32 point-kernel solver (checks,
+ * A/B timing).  FP64 and dense solvers always use the CUDA-core kernels. */
+mbc_status mbc_solver_set_matvec(mbc_solver *s, int32_t impl);
 
 typedef enum {
   MBC_SCHED_BATCHED = 0, /* all R columns advance together (per-column alpha, beta, stop) */
@@ -142,8 +153,8 @@ typedef struct {
   double tol;            /* stop when |r|^2 < tol^2 |b|^2, b = K^T f (kl_chol.cu:955) */
   int32_t schedule;      /* mbc_schedule */
   int32_t precondition;  /* 1 = KL preconditioner (the reference always passes true) */
-  int32_t max_refine;    /* MBC_F32: outer FP64 refinement sweeps (>= 1) */
-  double inner_tol;      /* MBC_F32: relative tolerance of each inner sweep */
+  int32_t max_refine;    /* MBC_F32: max FP64 residual replacements (0 = plain FP32 PCG) */
+  double inner_tol;      /* MBC_F32: replace once |r| fell by this factor since the last one */
   int32_t check_every;   /* iterations between convergence checks on the host */
   int32_t true_residual; /* 1 = report the FP64-recomputed |K^T(f-Kx)|/|K^T f| */
   int32_t profile;       /* 1 = time the matvec kernels with CUDA events on `stream` */
