@@ -46,8 +46,9 @@ class Plan:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and _lib._lib is not None:
-            _lib._lib.mbc_plan_destroy(h)
+        L = getattr(_lib, "_lib", None) if _lib is not None else None
+        if h and L is not None:
+            L.mbc_plan_destroy(h)
             self._h = None
 
     def order(self):
@@ -128,8 +129,9 @@ class Solver:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and _lib._lib is not None:
-            _lib._lib.mbc_solver_destroy(h)
+        L = getattr(_lib, "_lib", None) if _lib is not None else None
+        if h and L is not None:
+            L.mbc_solver_destroy(h)
             self._h = None
 
     def factor(self):

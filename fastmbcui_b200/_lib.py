@@ -51,7 +51,8 @@ class SolveStats(C.Structure):
                 ("iters_total", C.c_int64), ("refinements", C.c_int32),
                 ("n_converged", C.c_int32), ("relres_max", C.c_double),
                 ("true_relres_max", C.c_double), ("t_solve_ms", C.c_double),
-                ("t_matvec_ms", C.c_double), ("n_matvec", C.c_int64), ("kernel_launches", C.c_int64)]
+                ("t_matvec_ms", C.c_double), ("n_matvec", C.c_int64), ("kernel_launches", C.c_int64),
+                ("n_polished", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

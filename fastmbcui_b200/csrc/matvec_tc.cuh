@@ -4,24 +4,41 @@
 //   columns: T[j, r] = coef sum_i G(x_i, n_i, y_j) W[i, r]   (M = sources, K = rows)
 //
 // G = ((x - y).n) / |x - y|^3 is generated by SIMT warps tile by tile and
-// never stored.  One CTA owns 128 outputs (the MMA M) and all R columns (the
-// MMA N, R padded to a multiple of 16, at most 256); its accumulator lives in
-// tensor memory.  Per k-step of 32:
-//   * 8 producer warps evaluate the 128 x 32 tile of G in FP32, split each
-//     value into TF32 hi + lo (hi = rna(v), lo = rna(v - hi)), and stage the
-//     vector block (R x 32) the same way; both are stored K-major with the
-//     128-byte swizzle the MMA descriptors expect;
-//   * one thread issues 4 x 3 tcgen05.mma.kind::tf32 (K = 8 each):
-//     hi*hi + hi*lo + lo*hi ("3xTF32"), which keeps FP32-level accuracy;
-//   * a 2-stage ring of mbarriers (full: producers -> MMA, empty: MMA commit
-//     -> producers) overlaps generation with the tensor pipe.
-// The epilogue drains TMEM with tcgen05.ld (warps 0-3, one lane quarter
-// each), scales by coef and stores; the columns direction also forms the PCG
-// curvature partials p.t per CTA.
+// never stored; the vector block is the MMA's B operand.  Accuracy is FP32
+// level through "3xTF32": every operand value v is split into TF32 parts
+// hi = rna(v), lo = rna(v - hi), and D += A_lo B_hi + A_hi B_lo + A_hi B_hi
+// (the products are exact).  The tensor core's FP32 accumulation drops low
+// bits with a bias, so an accumulator that absorbs the whole reduction
+// drifts linearly with its length (measured: 2e-4 relative after 40000
+// terms, against 4e-6 for round-to-nearest FMAs).  The reduction is therefore
+// accumulated in chunks of kChunk k-steps: accumulator warps fold each
+// finished chunk into a second tensor-memory region with round-to-nearest
+// FP32 adds, which keeps the error at the level of an FP32 FMA loop.
 //
-// Every mbarrier wait is bounded: on expiry the kernel sets *err, stops
-// waiting, still commits its issued MMAs to the final barrier, frees its
-// tensor memory and returns.
+// Per launch:
+//   pack_b_kernel: the vector block, split into hi / lo and laid out per
+//     k-step exactly as the shared-memory image the MMA reads (K-major,
+//     128-byte swizzle), so a stage is one contiguous bulk copy.
+//   pk_tc_kernel: one CTA owns 128 outputs (accumulator of 128 lanes x np
+//     columns in tensor memory; np = R padded to 16) and walks the k-steps of
+//     32 through a 2-stage ring:
+//       loader warp  -- waits "empty", bulk-copies the stage's coordinates
+//                       and B image (cp.async.bulk, completion on "tma_full");
+//       8 producer warps -- wait "tma_full", evaluate the 128 x 32 tile of G
+//                       in FP32 from the staged coordinates, split, store
+//                       A hi / lo swizzled, fence to the async proxy, arrive
+//                       on "a_full";
+//       MMA warp     -- waits "a_full" (and, at a chunk start, "chunk_free"),
+//                       issues 4 x 3 tcgen05.mma (kind::tf32, K = 8),
+//                       commits to "empty" and, at a chunk end, "chunk_full";
+//       4 accumulator warps -- wait "chunk_full", add the chunk into the
+//                       running sum (tcgen05.ld / st), arrive "chunk_free";
+//                       after the last chunk they scale by coef and store,
+//                       and in the columns direction form the PCG curvature
+//                       partials p.t per CTA.
+// Every mbarrier wait is bounded: on expiry the kernel records the failure in
+// *err, stops waiting, releases the waiters it feeds, waits (bounded) for its
+// own copies, frees its tensor memory and returns.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -32,29 +49,45 @@
 namespace mbc {
 namespace tc {
 
-constexpr int kM = 128;        // MMA M (outputs per CTA)
-constexpr int kK = 32;         // k-step (one 128-byte swizzle row of TF32)
+constexpr int kM = 128;     // MMA M (outputs per CTA)
+constexpr int kK = 32;      // k-step: one 128-byte swizzle row of TF32
 constexpr int kStages = 2;
+constexpr int kChunk = 32;  // k-steps accumulated in tensor memory before a fold
 constexpr int kProducerWarps = 8;
-constexpr int kThreads = (kProducerWarps + 1) * 32;  // + the MMA warp
-constexpr uint32_t kWaitLimit = 1u << 22;            // polls of a bounded wait
+constexpr int kLoaderWarp = kProducerWarps;
+constexpr int kMmaWarp = kProducerWarps + 1;
+constexpr int kAccWarp0 = kProducerWarps + 2;  // 4 accumulator warps
+constexpr int kThreads = (kProducerWarps + 6) * 32;
+constexpr uint32_t kWaitLimit = 1u << 22;  // polls of a bounded wait
 
-constexpr int kTileA = kM * kK * 4;  // bytes of one A operand tile (16 KB)
+constexpr int kTileA = kM * kK * 4;  // one A operand tile: 16 KB
 
 __host__ __device__ constexpr int tile_b_bytes(int np) { return np * kK * 4; }
-__host__ __device__ constexpr int stage_bytes(int np) { return 2 * kTileA + 2 * tile_b_bytes(np); }
-// dynamic shared memory: 1 KB alignment slack + stages + 256 B of barriers
-// + the epilogue's per-warp partial sums (4 warps x 256 columns x 8 B)
-__host__ __device__ constexpr int smem_bytes(int np) { return 1024 + kStages * stage_bytes(np) + 256 + 8192; }
+__host__ __device__ constexpr int coord_bytes(int dir) { return dir == 0 ? kK * 16 : kK * 32; }
+__host__ __device__ constexpr int stage_bytes(int np, int dir)
+{
+  return 2 * kTileA + 2 * tile_b_bytes(np) + coord_bytes(dir);
+}
+// stages + 128 B of barriers + the accumulator warps' partial sums
+// (4 warps x 256 columns x 8 B); the dynamic shared window starts 1024-aligned
+__host__ __device__ constexpr int smem_bytes(int np, int dir)
+{
+  return kStages * stage_bytes(np, dir) + 128 + 8192;
+}
+
+__host__ __device__ constexpr int tmem_cols_for(int np)
+{
+  return np <= 32 ? 32 : np <= 64 ? 64 : np <= 128 ? 128 : 256;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// byte offset of element (row, k) in a K-major, 128B-swizzled tile whose
-// rows are 32 TF32 values (128 B); the tile base is 1024-byte aligned
-__device__ __forceinline__ uint32_t sw128(int row, int k)
+// byte offset of element (row, k) in a K-major, 128B-swizzled tile whose rows
+// are 32 TF32 values (128 B); tiles are 1024-byte aligned
+__host__ __device__ __forceinline__ uint32_t sw128(int row, int k)
 {
   return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((((k >> 2) ^ (row & 7)) & 7) << 4) +
                     ((k & 3) << 2));
@@ -81,6 +114,12 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
 }
 
 // bounded wait for the phase with the given parity; false on expiry
@@ -110,6 +149,16 @@ __device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity)
   got = __shfl_sync(0xffffffffu, got, 0);
   __syncwarp();
   return got != 0;
+}
+
+// global -> shared bulk copy completing on an mbarrier (16-byte aligned, size % 16 == 0)
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
 }
 
 __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr)
@@ -165,73 +214,126 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
   for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
 }
 
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32])
+{
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+      "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+      "r"(__float_as_uint(v[15])), "r"(__float_as_uint(v[16])), "r"(__float_as_uint(v[17])),
+      "r"(__float_as_uint(v[18])), "r"(__float_as_uint(v[19])), "r"(__float_as_uint(v[20])),
+      "r"(__float_as_uint(v[21])), "r"(__float_as_uint(v[22])), "r"(__float_as_uint(v[23])),
+      "r"(__float_as_uint(v[24])), "r"(__float_as_uint(v[25])), "r"(__float_as_uint(v[26])),
+      "r"(__float_as_uint(v[27])), "r"(__float_as_uint(v[28])), "r"(__float_as_uint(v[29])),
+      "r"(__float_as_uint(v[30])), "r"(__float_as_uint(v[31]))
+      : "memory");
+}
+
+// The B image: for each k-step ks, [hi tile | lo tile], each np rows x 128 B
+// laid out by sw128; element (r, k) = vin[(32 ks + k) * R + r], zero outside.
+// One thread per (k-step, row r, group of 4 k).
+__global__ void pack_b_kernel(const float *__restrict__ vin, int K_total, int R, int np, int nks,
+                              uint4 *__restrict__ img, const int32_t *__restrict__ done)
+{
+  if (done && *done) return;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t per_ks = (int64_t)np * (kK / 4);
+  if (t >= per_ks * nks) return;
+  const int ks = (int)(t / per_ks);
+  const int rem = (int)(t - (int64_t)ks * per_ks);
+  const int r = rem % np, kq = rem / np;
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int gk = ks * kK + kq * 4 + e;
+    const float v = (r < R && gk < K_total) ? vin[(size_t)gk * R + r] : 0.f;
+    split_tf32(v, h[e], l[e]);
+  }
+  unsigned char *base = reinterpret_cast<unsigned char *>(img) + (size_t)ks * 2 * tile_b_bytes(np);
+  const uint32_t off = sw128(r, kq * 4);
+  *reinterpret_cast<uint4 *>(base + off) = make_uint4(h[0], h[1], h[2], h[3]);
+  *reinterpret_cast<uint4 *>(base + tile_b_bytes(np) + off) = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
 struct TcArgs {
-  const float4 *xr, *nr;  // collocation rows (original order)
-  const float4 *ys;       // sources (new order)
+  const float4 *xr, *nr;  // collocation rows (original order), padded to 32
+  const float4 *ys;       // sources (new order), padded to 32
   int nf, n;
-  const float *vin;       // rows: V (n x R); columns: W (nf x R)
+  const uint4 *bimg;      // packed B image of the input block
   float *out;             // rows: W (nf x R); columns: T (n x R)
   int R, np;              // columns and padded MMA N (multiple of 16, <= 256)
-  int tmem_cols;          // power of two >= np, >= 32
+  int tmem_cols;          // per region: power of two >= np, >= 32
   float coef;
   const float *pdot;      // columns: p (n x R) for the curvature partials, or NULL
   double *part;           // columns: per-CTA partials (gridDim.x x R)
   const int32_t *done;    // PCG all-stopped flag (may be NULL)
-  int32_t *err;           // set to 1 when a bounded wait expires
+  int32_t *err;           // 1: a bounded wait expired; 2: shared memory misaligned
 };
 
 template <int DIR>
 __global__ void __launch_bounds__(kThreads, 1) pk_tc_kernel(TcArgs a)
 {
   if (a.done && *a.done) return;
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  const uint32_t raw = smem_u32(smem_raw);
-  unsigned char *base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
-  const int sb = stage_bytes(a.np);
-  unsigned char *tail = base + kStages * sb;
-  uint64_t *full = reinterpret_cast<uint64_t *>(tail);
-  uint64_t *empty = full + kStages;
-  uint64_t *done_bar = empty + kStages;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done_bar + 1);
+  extern __shared__ __align__(1024) unsigned char smem[];
+  if (smem_u32(smem) & 1023u) {
+    if (threadIdx.x == 0) atomicExch(a.err, 2);
+    return;
+  }
+  const int sb = stage_bytes(a.np, DIR);
+  const int btile = tile_b_bytes(a.np);
+  unsigned char *tail = smem + kStages * sb;
+  uint64_t *tma_full = reinterpret_cast<uint64_t *>(tail);
+  uint64_t *a_full = tma_full + kStages;
+  uint64_t *empty = a_full + kStages;
+  uint64_t *chunk_full = empty + kStages;
+  uint64_t *chunk_free = chunk_full + 1;
+  uint64_t *mma_done = chunk_free + 1;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mma_done + 1);
   int *s_fail = reinterpret_cast<int *>(tmem_slot + 1);
-  double *s_red = reinterpret_cast<double *>(tail + 256);  // [4][R] warp partials (columns)
+  double *s_red = reinterpret_cast<double *>(tail + 128);  // [4][R]
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int M_total = DIR == 0 ? a.nf : a.n;
   const int K_total = DIR == 0 ? a.n : a.nf;
   const int m0 = blockIdx.x * kM;
   const int nks = (K_total + kK - 1) / kK;
+  const int nchunks = (nks + kChunk - 1) / kChunk;
+  const int tcols = 2 * a.tmem_cols;  // [chunk accumulator | running sum]
 
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full[s], kProducerWarps);
+      mbar_init(&tma_full[s], 1);
+      mbar_init(&a_full[s], kProducerWarps);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(done_bar, 1);
+    mbar_init(chunk_full, 1);
+    mbar_init(chunk_free, 4);
+    mbar_init(mma_done, 1);
     *s_fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(a.tmem_cols)
+                 "r"(tcols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  // B rows np > R stay zero: clear every stage's B tiles once
-  for (int s = 0; s < kStages; ++s) {
-    uint4 *b = reinterpret_cast<uint4 *>(base + s * sb + 2 * kTileA);
-    for (int t = tid; t < 2 * tile_b_bytes(a.np) / 16; t += kThreads) b[t] = make_uint4(0, 0, 0, 0);
-  }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const uint32_t tmem_d = *tmem_slot;
+  const uint32_t tmem_acc = *tmem_slot;
+  const uint32_t tmem_sum = tmem_acc + (uint32_t)a.tmem_cols;
 
   if (warp < kProducerWarps) {
-    // ---------------- producers ----------------
-    const int row = (warp & 3) * 32 + lane;  // A row (output) owned by this thread
-    const int khalf = warp >> 2;             // which 16 of the 32 k
+    // ---------------- producers: the G tile ----------------
+    // row 32*(warp%4) + lane, k half warp/4 (16 values per k-step)
+    const int row = (warp & 3) * 32 + lane;
+    const int kbeg = (warp >> 2) * 16;
     const int gm = m0 + row;
     float4 own = make_float4(0.f, 0.f, 0.f, 0.f), own_n = own;
     if (gm < M_total) {
@@ -242,123 +344,174 @@ __global__ void __launch_bounds__(kThreads, 1) pk_tc_kernel(TcArgs a)
         own = a.ys[gm];
       }
     }
-    bool ok = true;
-    for (int ks = 0; ks < nks && ok; ++ks) {
+    for (int ks = 0; ks < nks; ++ks) {
       const int s = ks % kStages;
-      if (!mbar_wait_warp(&empty[s], ((ks / kStages) & 1) ^ 1)) {
-        ok = false;
+      if (!mbar_wait_warp(&tma_full[s], (ks / kStages) & 1)) {
+        *s_fail = 1;
         break;
       }
-      unsigned char *st = base + s * sb;
+      unsigned char *st = smem + s * sb;
       unsigned char *Ahi = st, *Alo = st + kTileA;
-      unsigned char *Bhi = st + 2 * kTileA, *Blo = Bhi + tile_b_bytes(a.np);
+      const float4 *co = reinterpret_cast<const float4 *>(st + 2 * kTileA + 2 * btile);
       const int k0 = ks * kK;
-      // A: 16 values of this thread's row
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         uint32_t h[4], l[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
-          const int k = khalf * 16 + q * 4 + e;
-          const int gk = k0 + k;
+          const int k = kbeg + q * 4 + e;
           float g = 0.f;
-          if (gk < K_total && gm < M_total) {
-            if (DIR == 0) g = PointKernel<float>::eval(own, own_n, __ldg(a.ys + gk));
-            else g = PointKernel<float>::eval(__ldg(a.xr + gk), __ldg(a.nr + gk), own);
+          if (gm < M_total && k0 + k < K_total) {
+            if (DIR == 0) g = PointKernel<float>::eval(own, own_n, co[k]);
+            else g = PointKernel<float>::eval(co[k], co[kK + k], own);
           }
           split_tf32(g, h[e], l[e]);
         }
-        const uint32_t off = sw128(row, khalf * 16 + q * 4);
+        const uint32_t off = sw128(row, kbeg + q * 4);
         *reinterpret_cast<uint4 *>(Ahi + off) = make_uint4(h[0], h[1], h[2], h[3]);
         *reinterpret_cast<uint4 *>(Alo + off) = make_uint4(l[0], l[1], l[2], l[3]);
       }
-      // B: chunks of 4 consecutive k of one column r; element (r, k) = vin[k0 + k][r]
-      const int nchunk = a.R * (kK / 4);
-      for (int c = tid; c < nchunk; c += kProducerWarps * 32) {
-        const int r = c % a.R, kq = c / a.R;
-        uint32_t h[4], l[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int gk = k0 + kq * 4 + e;
-          const float v = gk < K_total ? __ldg(a.vin + (size_t)gk * a.R + r) : 0.f;
-          split_tf32(v, h[e], l[e]);
-        }
-        const uint32_t off = sw128(r, kq * 4);
-        *reinterpret_cast<uint4 *>(Bhi + off) = make_uint4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<uint4 *>(Blo + off) = make_uint4(l[0], l[1], l[2], l[3]);
-      }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
-      if (lane == 0) mbar_arrive(&full[s]);
+      if (lane == 0) mbar_arrive(&a_full[s]);
     }
-    if (!ok) *s_fail = 1;
-  } else if (lane == 0) {
+  } else if (warp == kLoaderWarp) {
+    // ---------------- loader: coordinates + B image by bulk copy ----------------
+    if (lane == 0) {
+      const uint32_t cbytes = coord_bytes(DIR);
+      const uint32_t bbytes = 2 * btile;
+      int issued = 0;
+      for (int ks = 0; ks < nks; ++ks) {
+        const int s = ks % kStages;
+        if (!mbar_wait_one(&empty[s], ((ks / kStages) & 1) ^ 1)) {
+          *s_fail = 1;
+          break;
+        }
+        unsigned char *st = smem + s * sb;
+        unsigned char *bdst = st + 2 * kTileA;
+        unsigned char *cdst = bdst + 2 * btile;
+        const int k0 = ks * kK;
+        mbar_arrive_tx(&tma_full[s], cbytes + bbytes);
+        bulk_g2s(bdst, reinterpret_cast<const unsigned char *>(a.bimg) + (size_t)ks * bbytes, bbytes,
+                 &tma_full[s]);
+        if (DIR == 0) {
+          bulk_g2s(cdst, a.ys + k0, cbytes, &tma_full[s]);
+        } else {
+          // the 32 rows' points, then their normals
+          bulk_g2s(cdst, a.xr + k0, cbytes / 2, &tma_full[s]);
+          bulk_g2s(cdst + cbytes / 2, a.nr + k0, cbytes / 2, &tma_full[s]);
+        }
+        ++issued;
+      }
+      // no copy may still be landing when the CTA exits
+      for (int ks = issued > kStages ? issued - kStages : 0; ks < issued; ++ks)
+        if (!mbar_wait_one(&tma_full[ks % kStages], (ks / kStages) & 1)) *s_fail = 1;
+    }
+  } else if (warp == kMmaWarp) {
     // ---------------- MMA issue ----------------
-    const uint32_t idesc = idesc_tf32(a.np);
-    for (int ks = 0; ks < nks; ++ks) {
-      const int s = ks % kStages;
-      if (!mbar_wait_one(&full[s], (ks / kStages) & 1)) {
-        *s_fail = 1;
+    if (lane == 0) {
+      const uint32_t idesc = idesc_tf32(a.np);
+      bool broke = false;
+      for (int ks = 0; ks < nks; ++ks) {
+        const int s = ks % kStages;
+        const int kc = ks % kChunk;
+        // a new chunk overwrites the accumulator: the previous one must be folded
+        if (kc == 0 && ks > 0 && !mbar_wait_one(chunk_free, ((ks / kChunk) - 1) & 1)) {
+          *s_fail = 1;
+          broke = true;
+          break;
+        }
+        if (!mbar_wait_one(&a_full[s], (ks / kStages) & 1) ||
+            !mbar_wait_one(&tma_full[s], (ks / kStages) & 1)) {
+          *s_fail = 1;
+          broke = true;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t st = smem_u32(smem + s * sb);
+        const uint32_t Ahi = st, Alo = st + kTileA;
+        const uint32_t Bhi = st + 2 * kTileA, Blo = Bhi + btile;
+#pragma unroll
+        for (int kk = 0; kk < kK / 8; ++kk) {
+          const uint32_t ko = kk * 32;  // 8 TF32 = 32 bytes along the swizzled row
+          const uint32_t acc0 = (kc > 0 || kk > 0) ? 1u : 0u;
+          mma_tf32(tmem_acc, desc_sw128(Alo + ko), desc_sw128(Bhi + ko), idesc, acc0);
+          mma_tf32(tmem_acc, desc_sw128(Ahi + ko), desc_sw128(Blo + ko), idesc, 1u);
+          mma_tf32(tmem_acc, desc_sw128(Ahi + ko), desc_sw128(Bhi + ko), idesc, 1u);
+        }
+        mma_commit(&empty[s]);
+        if (kc == kChunk - 1 || ks == nks - 1) mma_commit(chunk_full);
+      }
+      // after an early exit, release the accumulator warps once every MMA
+      // issued so far has finished
+      if (broke) mma_commit(chunk_full);
+      // tensor memory is freed only after every issued MMA has finished
+      mma_commit(mma_done);
+      if (!mbar_wait_one(mma_done, 0)) *s_fail = 1;
+    }
+  } else {
+    // ---------------- accumulator warps: fold chunks, then the epilogue ----------------
+    const int q = warp & 3;  // tensor-memory lane quarter of this warp
+    const int gm = m0 + q * 32 + lane;
+    const uint32_t lane_off = (uint32_t)(q * 32) << 16;
+    bool ok = true;
+    for (int c = 0; c < nchunks; ++c) {
+      if (!mbar_wait_warp(chunk_full, c & 1)) {
+        ok = false;
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t st = smem_u32(base + s * sb);
-      const uint32_t Ahi = st, Alo = st + kTileA;
-      const uint32_t Bhi = st + 2 * kTileA, Blo = Bhi + tile_b_bytes(a.np);
+      const bool last = c == nchunks - 1;
+      for (int c0 = 0; c0 < a.np; c0 += 32) {
+        float v[32];
+        tmem_ld32(tmem_acc + lane_off + (uint32_t)c0, v);
+        if (c > 0) {
+          float u[32];
+          tmem_ld32(tmem_sum + lane_off + (uint32_t)c0, u);
 #pragma unroll
-      for (int kk = 0; kk < kK / 8; ++kk) {
-        const uint32_t ko = kk * 32;  // 8 TF32 = 32 bytes along the swizzled row
-        const uint32_t acc0 = (ks > 0 || kk > 0) ? 1u : 0u;
-        mma_tf32(tmem_d, desc_sw128(Alo + ko), desc_sw128(Bhi + ko), idesc, acc0);
-        mma_tf32(tmem_d, desc_sw128(Ahi + ko), desc_sw128(Blo + ko), idesc, 1u);
-        mma_tf32(tmem_d, desc_sw128(Ahi + ko), desc_sw128(Bhi + ko), idesc, 1u);
-      }
-      mma_commit(&empty[s]);
-    }
-    // completes when every MMA issued above has finished
-    mma_commit(done_bar);
-  }
-
-  // ---------------- epilogue: warps 0-3 ----------------
-  if (warp < 4) {
-    const bool have = mbar_wait_warp(done_bar, 0);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!have) *s_fail = 1;
-    const int row = warp * 32 + lane;
-    const int gm = m0 + row;
-    for (int c0 = 0; c0 < a.np; c0 += 32) {
-      float v[32];
-      tmem_ld32(tmem_d + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-      if (have && gm < M_total) {
-        float *o = a.out + (size_t)gm * a.R;
+          for (int k = 0; k < 32; ++k) v[k] += u[k];
+        }
+        if (!last) {
+          tmem_st32(tmem_sum + lane_off + (uint32_t)c0, v);
+          continue;
+        }
+        if (gm < M_total) {
+          float *o = a.out + (size_t)gm * a.R;
 #pragma unroll
-        for (int k = 0; k < 32; ++k)
-          if (c0 + k < a.R) o[c0 + k] = a.coef * v[k];
-      }
-      if (DIR == 1 && a.part) {
+          for (int k = 0; k < 32; ++k)
+            if (c0 + k < a.R) o[c0 + k] = a.coef * v[k];
+        }
+        if (DIR == 1 && a.part) {
 #pragma unroll
-        for (int k = 0; k < 32; ++k) {
-          double d = 0.0;
-          if (have && gm < M_total && c0 + k < a.R)
-            d = (double)(a.coef * v[k]) * (double)a.pdot[(size_t)gm * a.R + c0 + k];
+          for (int k = 0; k < 32; ++k) {
+            double d = 0.0;
+            if (gm < M_total && c0 + k < a.R)
+              d = (double)(a.coef * v[k]) * (double)a.pdot[(size_t)gm * a.R + c0 + k];
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
-          if (lane == 0 && c0 + k < a.R) s_red[warp * a.R + c0 + k] = d;
+            for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+            if (lane == 0 && c0 + k < a.R) s_red[q * a.R + c0 + k] = d;
+          }
         }
       }
+      if (!last) {
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(chunk_free);
+      }
     }
+    if (!ok) *s_fail = 1;
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (DIR == 1 && a.part && tid < a.R) {
     a.part[(size_t)blockIdx.x * a.R + tid] =
-        s_red[tid] + s_red[a.R + tid] + s_red[2 * a.R + tid] + s_red[3 * a.R + tid];
+        *s_fail ? 0.0 : s_red[tid] + s_red[a.R + tid] + s_red[2 * a.R + tid] + s_red[3 * a.R + tid];
   }
   if (tid == 0 && *s_fail && a.err) atomicExch(a.err, 1);
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(a.tmem_cols)
-                 : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_acc), "r"(tcols) : "memory");
   }
 }
 

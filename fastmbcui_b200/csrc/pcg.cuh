@@ -11,11 +11,15 @@
 
 namespace mbc {
 
-enum ColStatus : int32_t { COL_ACTIVE = -1, COL_OK = 0, COL_MAXIT = 1, COL_BREAKDOWN = 2 };
+// COL_STAGNANT: replacement mode only -- three consecutive replacements
+// found the true residual less than halved: the FP32 recursion has reached
+// its attainable accuracy and the column is finished in FP64.
+enum ColStatus : int32_t { COL_ACTIVE = -1, COL_OK = 0, COL_MAXIT = 1, COL_BREAKDOWN = 2, COL_STAGNANT = 3 };
 
 struct PcgScalars {
   double *rz, *b2, *thr, *alpha, *beta, *rr, *pt;
   double *rr_ref;  // residual replacement: |r|^2 at the last replacement
+  int32_t *stall;  // residual replacement: consecutive replacements without progress
   int32_t *status, *iters;
   int32_t *done;   // 1 when no column is active
   int32_t *want;   // residual replacement requested (set by RED_CHECK)
@@ -164,6 +168,7 @@ __global__ void __launch_bounds__(1024) reduce_kernel(int nblk, int R,
           sc.b2[c] = s;
           sc.thr[c] = sc.tol2 * s;
           if (sc.rr_ref) sc.rr_ref[c] = s;
+          if (sc.stall) sc.stall[c] = 0;
           if (sc.status[c] == COL_ACTIVE && s < 1e-16) {
             sc.status[c] = COL_OK;  // kl_chol.cu:950-953: zero right-hand side
             sc.rr[c] = 0.0;
@@ -202,10 +207,17 @@ __global__ void __launch_bounds__(1024) reduce_kernel(int nblk, int R,
           break;
         case RED_REPLACE:
           if (sc.status[c] == COL_ACTIVE || sc.status[c] == COL_MAXIT) {
+            const double prev = sc.rr_ref[c];
             sc.rr[c] = s;
             sc.rr_ref[c] = s;
-            if (!(s == s)) sc.status[c] = COL_BREAKDOWN;
-            else if (s < sc.thr[c]) sc.status[c] = COL_OK;
+            if (!(s == s)) {
+              sc.status[c] = COL_BREAKDOWN;
+            } else if (s < sc.thr[c]) {
+              sc.status[c] = COL_OK;
+            } else {
+              sc.stall[c] = s > 0.25 * prev ? sc.stall[c] + 1 : 0;
+              if (sc.stall[c] >= 3 && sc.status[c] == COL_ACTIVE) sc.status[c] = COL_STAGNANT;
+            }
           }
           break;
         case RED_BETA:
@@ -272,6 +284,28 @@ __global__ void accumulate_kernel(int n, int R, const T *__restrict__ d, double 
 {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx < (int64_t)n * R) x[idx] += (double)d[idx];
+}
+
+// dst[i, k] = src[i, idx[k]]   (n rows, R -> Rs columns)
+template <typename T>
+__global__ void gather_cols_kernel(int n, int R, int Rs, const int32_t *__restrict__ idx,
+                                   const T *__restrict__ src, T *__restrict__ dst)
+{
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)n * Rs) return;
+  const int i = (int)(t / Rs), k = (int)(t - (int64_t)i * Rs);
+  dst[t] = src[(size_t)i * R + idx[k]];
+}
+
+// dst[i, idx[k]] = src[i, k]
+template <typename T>
+__global__ void scatter_cols_kernel(int n, int R, int Rs, const int32_t *__restrict__ idx,
+                                    const T *__restrict__ src, T *__restrict__ dst)
+{
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)n * Rs) return;
+  const int i = (int)(t / Rs), k = (int)(t - (int64_t)i * Rs);
+  dst[(size_t)i * R + idx[k]] = src[t];
 }
 
 // points (n x 3 float, stride 3) -> float4, optionally gathered by `order`

@@ -143,40 +143,49 @@ int cols_launch(const Solver &S, int R, const T *w, T *t, const T *pdot, double 
 
 }  // namespace
 
-// tensor-core path: FP32 point kernel, 8 <= R <= 256
+// tensor-core path: FP32 point kernel, R <= 256 (auto: R >= 8); needs the
+// packed B image buffer (falls back to the CUDA-core kernels without it)
 static bool use_tc(const Solver &S, int R)
 {
   if (S.op.kind != MBC_OP_POINT_KERNEL || R > 256) return false;
   if (S.matvec_impl == MBC_MATVEC_SIMT) return false;
-  if (S.matvec_impl == MBC_MATVEC_TENSOR) return true;
-  return R >= 8;
+  if (S.matvec_impl == MBC_MATVEC_AUTO && R < 8) return false;
+  const int np = (R + 15) / 16 * 16;
+  const int K = std::max(S.n, S.nf);
+  const size_t need = (size_t)cdiv(K, tc::kK) * 2 * tc::tile_b_bytes(np);
+  return S.m_bimg.reserve(need) == MBC_OK;
 }
 
 template <int DIR>
 static int tc_launch(const Solver &S, int R, const float *vin, float *out, const float *pdot,
                      double *part, const int32_t *done, cudaStream_t st)
 {
+  const int M = DIR == 0 ? S.nf : S.n;
+  const int K = DIR == 0 ? S.n : S.nf;
   tc::TcArgs a{};
   a.xr = S.x4();
   a.nr = S.n4();
   a.ys = S.y4();
   a.nf = S.nf;
   a.n = S.n;
-  a.vin = vin;
+  a.bimg = (const uint4 *)S.m_bimg.ptr;
   a.out = out;
   a.R = R;
   a.np = (R + 15) / 16 * 16;
-  a.tmem_cols = a.np <= 32 ? 32 : a.np <= 64 ? 64 : a.np <= 128 ? 128 : 256;
+  a.tmem_cols = tc::tmem_cols_for(a.np);
   a.coef = (float)S.op.coef;
   a.pdot = pdot;
   a.part = part;
   a.done = done;
   a.err = (int32_t *)S.m_err.ptr;
-  cudaFuncSetAttribute(tc::pk_tc_kernel<DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       tc::smem_bytes(256));
-  const int M = DIR == 0 ? S.nf : S.n;
+  const int nks = (int)cdiv(K, tc::kK);
+  const int64_t pack_threads = (int64_t)nks * a.np * (tc::kK / 4);
+  tc::pack_b_kernel<<<cdiv(pack_threads, 256), 256, 0, st>>>(vin, K, R, a.np, nks, (uint4 *)S.m_bimg.ptr,
+                                                              done);
+  const int smem = tc::smem_bytes(a.np, DIR);
+  cudaFuncSetAttribute(tc::pk_tc_kernel<DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   const unsigned grid = cdiv(M, tc::kM);
-  tc::pk_tc_kernel<DIR><<<grid, tc::kThreads, tc::smem_bytes(a.np), st>>>(a);
+  tc::pk_tc_kernel<DIR><<<grid, tc::kThreads, smem, st>>>(a);
   return (int)grid;
 }
 
@@ -427,9 +436,14 @@ mbc_status Solver::create(const Plan &pl, const mbc_operator &o, int32_t prec, c
   MBC_TRY(m_err.reserve(sizeof(int32_t)));
   MBC_CK(cudaMemsetAsync(m_err.ptr, 0, sizeof(int32_t), st));
   if (o.kind == MBC_OP_POINT_KERNEL) {
-    MBC_TRY(m_x4.reserve(sizeof(float4) * nf));
-    MBC_TRY(m_n4.reserve(sizeof(float4) * nf));
-    MBC_TRY(m_y4.reserve(sizeof(float4) * n));
+    // padded to whole 32-point tiles (the tensor-core path copies whole tiles)
+    const size_t nf_pad = (size_t)cdiv(nf, 32) * 32, n_pad = (size_t)cdiv(n, 32) * 32;
+    MBC_TRY(m_x4.reserve(sizeof(float4) * nf_pad));
+    MBC_TRY(m_n4.reserve(sizeof(float4) * nf_pad));
+    MBC_TRY(m_y4.reserve(sizeof(float4) * n_pad));
+    MBC_CK(cudaMemsetAsync(m_x4.ptr, 0, sizeof(float4) * nf_pad, st));
+    MBC_CK(cudaMemsetAsync(m_n4.ptr, 0, sizeof(float4) * nf_pad, st));
+    MBC_CK(cudaMemsetAsync(m_y4.ptr, 0, sizeof(float4) * n_pad, st));
     pack_points_kernel<<<cdiv(nf, 256), 256, 0, st>>>(nf, o.x, nullptr, (float4 *)m_x4.ptr);
     pack_points_kernel<<<cdiv(nf, 256), 256, 0, st>>>(nf, o.nx, nullptr, (float4 *)m_n4.ptr);
     pack_points_kernel<<<cdiv(n, 256), 256, 0, st>>>(n, o.y, (const int32_t *)m_Pinv.ptr,
@@ -495,7 +509,7 @@ static mbc_status pcg_buffers(Solver &S, int R, PcgWork<T> &w)
   w.part_stride = nblk;
   MBC_TRY(S.part.reserve(sizeof(double) * (size_t)nblk * R));
   w.part = (double *)S.part.ptr;
-  MBC_TRY(S.scal.reserve(sizeof(double) * 8 * R + sizeof(int32_t) * (2 * R + 4)));
+  MBC_TRY(S.scal.reserve(sizeof(double) * 8 * R + sizeof(int32_t) * (3 * R + 4)));
   double *d = (double *)S.scal.ptr;
   w.sc.rz = d;
   w.sc.b2 = d + R;
@@ -510,6 +524,7 @@ static mbc_status pcg_buffers(Solver &S, int R, PcgWork<T> &w)
   w.sc.iters = ii + R;
   w.sc.done = ii + 2 * R;
   w.sc.want = ii + 2 * R + 1;
+  w.sc.stall = ii + 2 * R + 4;
   w.sc.drop2 = 0.0;
   return MBC_OK;
 }
@@ -906,11 +921,59 @@ mbc_status Solver::solve_mixed(int R, const void *rhs, int32_t rhs_dt, void *X, 
   std::vector<int32_t> status, iters;
   std::vector<double> rel;
   MBC_TRY(collect<float>(*this, R, w, status, iters, rel, st));
+  const int32_t n_repl = replacements;
+  // columns the FP32 recursion could not finish (stagnant or out of
+  // iterations) are polished by FP64 PCG warm-started from their FP64 x
+  std::vector<int32_t> pol;
+  for (int c = 0; c < R; ++c)
+    if (status[c] == COL_STAGNANT || status[c] == COL_MAXIT) pol.push_back(c);
+  if (!pol.empty()) {
+    const int Rs = (int)pol.size();
+    MBC_TRY(polish_idx.reserve(sizeof(int32_t) * (Rs + 2) + sizeof(double) * R));
+    int32_t *d_idx = (int32_t *)polish_idx.ptr;
+    MBC_CK(cudaMemcpyAsync(d_idx, pol.data(), sizeof(int32_t) * Rs, cudaMemcpyHostToDevice, st));
+    PcgWork<double> w64;
+    MBC_TRY(pcg_buffers<double>(*this, Rs, w64));
+    const int64_t ns = (int64_t)n * Rs;
+    gather_cols_kernel<double><<<cdiv(ns, 256), 256, 0, st>>>(n, R, Rs, d_idx, Xd, w64.X);
+    gather_cols_kernel<double><<<cdiv(ns, 256), 256, 0, st>>>(n, R, Rs, d_idx, Rd, w64.Rv);
+    std::vector<double> b2_all(R), b2_sel(Rs);
+    MBC_CK(cudaMemcpyAsync(b2_all.data(), b2ref.ptr, sizeof(double) * R, cudaMemcpyDeviceToHost, st));
+    MBC_CK(cudaStreamSynchronize(st));
+    for (int k = 0; k < Rs; ++k) b2_sel[k] = b2_all[pol[k]];
+    double *d_b2s = (double *)((int32_t *)polish_idx.ptr + ((Rs + 1) & ~1));
+    MBC_CK(cudaMemcpyAsync(d_b2s, b2_sel.data(), sizeof(double) * Rs, cudaMemcpyHostToDevice, st));
+    launches += 2;
+    MBC_CKL();
+    MBC_TRY((run_pcg<double, float, double>(*this, Rs, w64, w64.X, (const float *)lval.ptr,
+                                            o.max_iters, o.tol, o.precondition != 0,
+                                            std::max(1, o.check_every), nullptr, st, d_b2s, nullptr,
+                                            0)));
+    std::vector<int32_t> it64(Rs);
+    MBC_CK(cudaMemcpyAsync(it64.data(), w64.sc.iters, sizeof(int32_t) * Rs, cudaMemcpyDeviceToHost, st));
+    scatter_cols_kernel<double><<<cdiv(ns, 256), 256, 0, st>>>(n, R, Rs, d_idx, w64.X, Xd);
+    ++launches;
+    MBC_CKL();
+    MBC_CK(cudaStreamSynchronize(st));
+    for (int k = 0; k < Rs; ++k) iters[pol[k]] += it64[k];
+    // judge every polished column on its FP64 true residual
+    MBC_TRY(true_residual_into_r());
+    std::vector<double> nr, nb;
+    MBC_TRY(col_norms2<double>(*this, R, Rd, nr, st));
+    MBC_TRY(col_norms2<double>(*this, R, Bd, nb, st));
+    for (int c : pol) {
+      rel[c] = nb[c] < 1e-16 ? 0.0 : std::sqrt(nr[c] / nb[c]);
+      status[c] = rel[c] <= o.tol ? COL_OK : COL_MAXIT;
+    }
+  }
   permute_out<double>(*this, R, Xd, X, x_dt, st);
   MBC_CKL();
+  for (int c = 0; c < R; ++c)
+    if (status[c] == COL_STAGNANT) status[c] = COL_MAXIT;
   MBC_TRY(finish_stats(R, status, iters, rel, stats, iters_host));
   if (stats) {
-    stats->refinements = replacements + 1;
+    stats->n_polished = (int32_t)pol.size();
+    stats->refinements = n_repl + 1;
     double m = 0;
     for (int c = 0; c < R; ++c) m = std::max(m, rel[c]);
     stats->true_relres_max = m;
@@ -1064,6 +1127,7 @@ mbc_status mbc::Solver::check_device_error(cudaStream_t st)
   MBC_CK(cudaStreamSynchronize(st));
   if (e) {
     MBC_CK(cudaMemsetAsync(m_err.ptr, 0, sizeof(int32_t), st));
+    if (e == 2) return fail(MBC_CUDA_ERROR, "tensor-core matvec: shared memory window not 1024-byte aligned");
     return fail(MBC_TIMEOUT, "a bounded device wait expired in the tensor-core matvec");
   }
   return MBC_OK;

@@ -42,11 +42,12 @@ struct Solver {
   DevMem class_list[4];
   // operator: rows (original order) and sources (new order) as float4
   DevMem m_x4, m_n4, m_y4;
-  DevMem m_err;  // set by a tensor-core kernel whose bounded wait expired
+  DevMem m_err;           // set by a tensor-core kernel (1: a bounded wait expired)
+  mutable DevMem m_bimg;  // packed TF32 hi/lo image of the tensor-core B operand
   // factor
   DevMem theta, theta64, lval, bad, fscratch;
   // PCG workspaces
-  DevMem work32, work64, part, scal, fbuf32, fbuf64, res64, mask, colbuf, tmp, b2ref, nrm;
+  DevMem work32, work64, part, scal, fbuf32, fbuf64, res64, mask, colbuf, tmp, b2ref, nrm, polish_idx;
 
   ~Solver();
 

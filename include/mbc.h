@@ -172,6 +172,8 @@ typedef struct {
   double t_matvec_ms;       /* profile: summed duration of the K and K^T kernels */
   int64_t n_matvec;         /* profile: K / K^T launches timed */
   int64_t kernel_launches;  /* kernels this call launched */
+  int32_t n_polished;       /* MBC_F32: columns finished by FP64 PCG after the FP32
+                               recursion stagnated or ran out of iterations */
 } mbc_solve_stats;
 
 void mbc_solve_default_options(mbc_solve_options *opt);

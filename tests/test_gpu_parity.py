@@ -106,6 +106,27 @@ def test_matvec_tensor_ragged_sizes():
         assert rel(s.apply_KT(_dev(W)).cpu().numpy(), c.op.KT(W)) < 2e-5
 
 
+@pytest.mark.parametrize("R", [48, 192])
+def test_matvec_tensor_long_reduction_vs_fp64(R):
+    # 40000-term reductions: the chunked tensor-memory accumulation must stay
+    # at FP32-FMA accuracy (an unchunked accumulator drifted to 2e-4)
+    sc = S.ellipsoids_scene(20, 2000, seed=12)
+    plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
+    s = F.Solver(plan, x=_dev(sc.x), nx=_dev(sc.nx), y=_dev(sc.y), coef=sc.coef, precision=F.MBC_F32)
+    s64 = F.Solver(plan, x=_dev(sc.x), nx=_dev(sc.nx), y=_dev(sc.y), coef=sc.coef, precision=F.MBC_F64)
+    rng = np.random.default_rng(R)
+    V = _dev(rng.standard_normal((sc.n, R)))
+    W = _dev(rng.standard_normal((sc.nf, R)))
+    gk = s64.apply_K(V.double()).cpu().numpy()
+    gkt = s64.apply_KT(W.double()).cpu().numpy()
+    s.set_matvec(F.MBC_MATVEC_TENSOR)
+    kt, ktt = s.apply_K(V).double().cpu().numpy(), s.apply_KT(W).double().cpu().numpy()
+    s.set_matvec(F.MBC_MATVEC_SIMT)
+    ks, kst = s.apply_K(V).double().cpu().numpy(), s.apply_KT(W).double().cpu().numpy()
+    assert rel(ks, gk) < 1e-5 and rel(kst, gkt) < 1e-5
+    assert rel(kt, gk) < 1e-5 and rel(ktt, gkt) < 1e-5
+
+
 @pytest.mark.parametrize("R", [1, 5, 33])
 def test_dense_matvec(ells, R):
     K32 = ells.sc.dense_K().astype(np.float32)
