@@ -85,6 +85,7 @@ SIGNATURES = {
                                     C.POINTER(SolveStats), _vp, _vp]),
     "mbc_apply_K": (C.c_int, [_vp, _i32, _vp, _vp, _vp]),
     "mbc_apply_KT": (C.c_int, [_vp, _i32, _vp, _vp, _vp]),
+    "mbc_point_apply_noalloc": (C.c_int, [_i32, _i32, _i32, _vp, _vp, _vp, C.c_double, _i32, _vp, _vp, _vp]),
     "mbc_context_create": (C.c_int, [C.POINTER(_vp)]),
     "mbc_context_destroy": (C.c_int, [_vp]),
     "mbc_context_last_stats": (C.c_int, [_vp, C.POINTER(SolveStats)]),

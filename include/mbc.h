@@ -198,6 +198,26 @@ mbc_status mbc_solve_adjoint(mbc_solver *s, int32_t R, const void *B, int32_t b_
 mbc_status mbc_apply_K(mbc_solver *s, int32_t R, const void *V, void *W, mbc_stream stream);
 mbc_status mbc_apply_KT(mbc_solver *s, int32_t R, const void *W, void *T, mbc_stream stream);
 
+/* Point-kernel matvec that allocates no device memory.  No counterpart in the
+ * reference: it serves callers that cannot let a library call cudaMalloc or
+ * cudaFree -- hosts that own the device through their own memory pool or a
+ * fixed memory budget (a simulation loop, a framework's caching allocator),
+ * where those calls can block on the whole device and fail late.
+ *   transpose 0: out (nf x R) = coef K in (n x R),  K(i,j) = ((x_i - y_j) . nx_i) / |x_i - y_j|^3
+ *   transpose 1: out (n x R)  = coef K^T in (nf x R)
+ * x, nx: device nf x 3 float32; y: device n x 3 float32; in, out: device
+ * row-major float32, ORIGINAL point order (no plan).  FP32 CUDA-core kernels.
+ * Workspace: a 4 MiB static device array inside this library, held on every
+ * GPU that loads it until exit; sizes with 2*ceil16(nf) + ceil16(n) > 262144
+ * are refused with MBC_BAD_ARG.  The first call on a device looks the array's
+ * address up (with that device current); make that first call before any
+ * stream capture.  All calls share the array and each rewrites the parts it
+ * reads, so calls whose kernels overlap on the GPU (different streams, or
+ * several host threads) race: serialise them. */
+mbc_status mbc_point_apply_noalloc(int32_t transpose, int32_t nf, int32_t n, const float *x,
+                                   const float *nx, const float *y, double coef, int32_t R,
+                                   const float *in, float *out, mbc_stream stream);
+
 /* ------------------------------------------------------------------------ */
 /* mfs_torch operator bodies (the drop-in).                                   */
 /* mbc_minvf_float replaces MinvF_float (mfs_torch/csrc/mfs_torch_ops.cu:21-197, */
