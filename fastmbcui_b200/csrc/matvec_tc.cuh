@@ -21,21 +21,24 @@
 //     128-byte swizzle), so a stage is one contiguous bulk copy.
 //   pk_tc_kernel: one CTA owns 128 outputs (accumulator of 128 lanes x np
 //     columns in tensor memory; np = R padded to 16) and walks the k-steps of
-//     32 through a 2-stage ring:
-//       loader warp  -- waits "empty", bulk-copies the stage's coordinates
-//                       and B image (cp.async.bulk, completion on "tma_full");
-//       8 producer warps -- wait "tma_full", evaluate the 128 x 32 tile of G
-//                       in FP32 from the staged coordinates, split, store
-//                       A hi / lo swizzled, fence to the async proxy, arrive
-//                       on "a_full";
-//       MMA warp     -- waits "a_full" (and, at a chunk start, "chunk_free"),
-//                       issues 4 x 3 tcgen05.mma (kind::tf32, K = 8),
-//                       commits to "empty" and, at a chunk end, "chunk_full";
-//       4 accumulator warps -- wait "chunk_full", add the chunk into the
-//                       running sum (tcgen05.ld / st), arrive "chunk_free";
-//                       after the last chunk they scale by coef and store,
-//                       and in the columns direction form the PCG curvature
-//                       partials p.t per CTA.
+//     32 through two shared-memory rings: 2 stages of A (the G tile, hi and
+//     lo) and 3 stages (2 when np > 192) of B image + coordinates, so the bulk
+//     copy of a step is issued two MMA steps before it is needed:
+//       loader warp  -- waits "bempty", bulk-copies the stage's coordinates
+//                       and B image (cp.async.bulk, completion on "bfull");
+//       16 producer warps -- wait "bfull" and "aempty", evaluate the 128 x 32
+//                       tile of G in FP32 from the staged coordinates, split,
+//                       store A hi / lo swizzled, fence to the async proxy,
+//                       arrive on "afull";
+//       MMA warp     -- waits "afull" and "bfull" (and, at a chunk start,
+//                       "chunk_free"), issues 4 x 3 tcgen05.mma (kind::tf32,
+//                       K = 8), commits to "aempty" and "bempty" and, at a
+//                       chunk end, "chunk_full";
+//       4 accumulator warps -- wait "chunk_full" (sleeping between polls),
+//                       add the chunk into the running sum (tcgen05.ld / st),
+//                       arrive "chunk_free"; after the last chunk they scale
+//                       by coef and store, and in the columns direction form
+//                       the PCG curvature partials p.t per CTA.
 // Every mbarrier wait is bounded: on expiry the kernel records the failure in
 // *err, stops waiting, releases the waiters it feeds, waits (bounded) for its
 // own copies, frees its tensor memory and returns.
@@ -51,28 +54,44 @@ namespace tc {
 
 constexpr int kM = 128;     // MMA M (outputs per CTA)
 constexpr int kK = 32;      // k-step: one 128-byte swizzle row of TF32
-constexpr int kStages = 2;
+constexpr int kAStages = 2;     // ring of produced A (G) tiles
+constexpr int kMaxBStages = 3;  // ring of bulk-copied B image + coordinates
 constexpr int kChunk = 32;  // k-steps accumulated in tensor memory before a fold
-constexpr int kProducerWarps = 8;
+constexpr int kProducerWarps = 16;
 constexpr int kLoaderWarp = kProducerWarps;
 constexpr int kMmaWarp = kProducerWarps + 1;
 constexpr int kAccWarp0 = kProducerWarps + 2;  // 4 accumulator warps
-constexpr int kThreads = (kProducerWarps + 6) * 32;
+constexpr int kSchedWarp = kProducerWarps + 6;
+constexpr int kThreads = (kProducerWarps + 7) * 32;
+// named barriers (0 is __syncthreads).  Every participant uses bar.sync, so
+// no role can run more than one step ahead of a partner.
+constexpr int kBarGo = 1;      // producers + scheduler warp, once per k-step
+constexpr int kBarAReady = 2;  // producers + MMA warp, once per k-step
+constexpr int kBarAcc = 3;     // the 4 accumulator warps, once per chunk
+constexpr int kGoCount = (kProducerWarps + 1) * 32;
+constexpr int kKPerProducer = kK / (kProducerWarps / 4);  // k values per row per k-step
 constexpr uint32_t kWaitLimit = 1u << 22;  // polls of a bounded wait
+constexpr int kSmemLimit = 232448;        // opt-in dynamic shared memory per CTA (227 KB)
+constexpr int kTail = 256 + 8192;         // barriers, then the accumulator warps' partials
 
 constexpr int kTileA = kM * kK * 4;  // one A operand tile: 16 KB
+constexpr int kABytes = kAStages * 2 * kTileA;
 
 __host__ __device__ constexpr int tile_b_bytes(int np) { return np * kK * 4; }
 __host__ __device__ constexpr int coord_bytes(int dir) { return dir == 0 ? kK * 16 : kK * 32; }
-__host__ __device__ constexpr int stage_bytes(int np, int dir)
+// one B stage: [B hi | B lo | coordinates], rounded so every tile stays 1024-aligned
+__host__ __device__ constexpr int bstage_bytes(int np, int dir)
 {
-  return 2 * kTileA + 2 * tile_b_bytes(np) + coord_bytes(dir);
+  return (2 * tile_b_bytes(np) + coord_bytes(dir) + 1023) / 1024 * 1024;
 }
-// stages + 128 B of barriers + the accumulator warps' partial sums
-// (4 warps x 256 columns x 8 B); the dynamic shared window starts 1024-aligned
+__host__ __device__ constexpr int b_stages(int np, int dir)
+{
+  return kABytes + kMaxBStages * bstage_bytes(np, dir) + kTail <= kSmemLimit ? kMaxBStages : 2;
+}
+// [A ring | B ring | tail]; the dynamic shared window starts 1024-aligned
 __host__ __device__ constexpr int smem_bytes(int np, int dir)
 {
-  return kStages * stage_bytes(np, dir) + 128 + 8192;
+  return kABytes + b_stages(np, dir) * bstage_bytes(np, dir) + kTail;
 }
 
 __host__ __device__ constexpr int tmem_cols_for(int np)
@@ -122,8 +141,10 @@ __device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes)
                : "memory");
 }
 
-// bounded wait for the phase with the given parity; false on expiry
-__device__ __forceinline__ bool mbar_wait_one(uint64_t *bar, uint32_t parity)
+// bounded wait for the phase with the given parity; false on expiry.  Roles
+// that wait long (sleep_ns > 0) back off between polls so that their polling
+// does not take issue slots from the producer warps.
+__device__ __forceinline__ bool mbar_wait_one(uint64_t *bar, uint32_t parity, uint32_t sleep_ns = 0)
 {
   const uint32_t a = smem_u32(bar);
   for (uint32_t it = 0; it < kWaitLimit; ++it) {
@@ -136,16 +157,17 @@ __device__ __forceinline__ bool mbar_wait_one(uint64_t *bar, uint32_t parity)
         : "r"(a), "r"(parity)
         : "memory");
     if (ok) return true;
+    if (sleep_ns) __nanosleep(sleep_ns);
   }
   return false;
 }
 
 // warp-uniform bounded wait: lane 0 polls, the outcome is broadcast and
 // __syncwarp orders the other lanes after lane 0's acquire
-__device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity, uint32_t sleep_ns = 0)
 {
   int got = 0;
-  if ((threadIdx.x & 31) == 0) got = mbar_wait_one(bar, parity) ? 1 : 0;
+  if ((threadIdx.x & 31) == 0) got = mbar_wait_one(bar, parity, sleep_ns) ? 1 : 0;
   got = __shfl_sync(0xffffffffu, got, 0);
   __syncwarp();
   return got != 0;
@@ -284,18 +306,22 @@ __global__ void __launch_bounds__(kThreads, 1) pk_tc_kernel(TcArgs a)
     if (threadIdx.x == 0) atomicExch(a.err, 2);
     return;
   }
-  const int sb = stage_bytes(a.np, DIR);
+  const int nbs = b_stages(a.np, DIR);
+  const int bst = bstage_bytes(a.np, DIR);
   const int btile = tile_b_bytes(a.np);
-  unsigned char *tail = smem + kStages * sb;
-  uint64_t *tma_full = reinterpret_cast<uint64_t *>(tail);
-  uint64_t *a_full = tma_full + kStages;
-  uint64_t *empty = a_full + kStages;
-  uint64_t *chunk_full = empty + kStages;
+  unsigned char *bring = smem + kABytes;
+  unsigned char *tail = bring + nbs * bst;
+  uint64_t *bfull = reinterpret_cast<uint64_t *>(tail);  // B stage landed
+  uint64_t *bempty = bfull + kMaxBStages;                 // B stage read by its MMAs
+  uint64_t *afull = bempty + kMaxBStages;                 // A stage written by the producers
+  uint64_t *aempty = afull + kAStages;                    // A stage read by its MMAs
+  uint64_t *chunk_full = aempty + kAStages;
   uint64_t *chunk_free = chunk_full + 1;
   uint64_t *mma_done = chunk_free + 1;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mma_done + 1);
   int *s_fail = reinterpret_cast<int *>(tmem_slot + 1);
-  double *s_red = reinterpret_cast<double *>(tail + 128);  // [4][R]
+  volatile int *s_aflag = s_fail + 1;  // [2]: chunk landed, as seen by the polling accumulator warp
+  double *s_red = reinterpret_cast<double *>(tail + 256);  // [4][R]
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int M_total = DIR == 0 ? a.nf : a.n;
@@ -306,10 +332,13 @@ __global__ void __launch_bounds__(kThreads, 1) pk_tc_kernel(TcArgs a)
   const int tcols = 2 * a.tmem_cols;  // [chunk accumulator | running sum]
 
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(&tma_full[s], 1);
-      mbar_init(&a_full[s], kProducerWarps);
-      mbar_init(&empty[s], 1);
+    for (int s = 0; s < kMaxBStages; ++s) {
+      mbar_init(&bfull[s], 1);
+      mbar_init(&bempty[s], 1);
+    }
+    for (int s = 0; s < kAStages; ++s) {
+      mbar_init(&afull[s], kProducerWarps);
+      mbar_init(&aempty[s], 1);
     }
     mbar_init(chunk_full, 1);
     mbar_init(chunk_free, 4);
@@ -329,11 +358,18 @@ __global__ void __launch_bounds__(kThreads, 1) pk_tc_kernel(TcArgs a)
   const uint32_t tmem_acc = *tmem_slot;
   const uint32_t tmem_sum = tmem_acc + (uint32_t)a.tmem_cols;
 
+  // Producers never poll an mbarrier: the scheduler warp polls "bfull" and
+  // "aempty" for step ks while the producers compute step ks - 1, and meets
+  // them at the "go" barrier; finished A stages reach the MMA warp through the
+  // "A ready" barrier.  Named barriers cannot time out, so every role takes all
+  // nks steps of its barrier sequence even after a failure (s_fail), doing no
+  // work in those steps.
+  volatile int *vfail = s_fail;
   if (warp < kProducerWarps) {
     // ---------------- producers: the G tile ----------------
-    // row 32*(warp%4) + lane, k half warp/4 (16 values per k-step)
+    // row 32*(warp%4) + lane, kKPerProducer values of each k-step
     const int row = (warp & 3) * 32 + lane;
-    const int kbeg = (warp >> 2) * 16;
+    const int kbeg = (warp >> 2) * kKPerProducer;
     const int gm = m0 + row;
     float4 own = make_float4(0.f, 0.f, 0.f, 0.f), own_n = own;
     if (gm < M_total) {
@@ -345,35 +381,43 @@ __global__ void __launch_bounds__(kThreads, 1) pk_tc_kernel(TcArgs a)
       }
     }
     for (int ks = 0; ks < nks; ++ks) {
-      const int s = ks % kStages;
-      if (!mbar_wait_warp(&tma_full[s], (ks / kStages) & 1)) {
-        *s_fail = 1;
-        break;
-      }
-      unsigned char *st = smem + s * sb;
-      unsigned char *Ahi = st, *Alo = st + kTileA;
-      const float4 *co = reinterpret_cast<const float4 *>(st + 2 * kTileA + 2 * btile);
-      const int k0 = ks * kK;
+      const int sa = ks % kAStages, sb = ks % nbs;
+      asm volatile("bar.sync %0, %1;" ::"n"(kBarGo), "n"(kGoCount) : "memory");
+      if (!*vfail) {
+        unsigned char *Ahi = smem + sa * 2 * kTileA, *Alo = Ahi + kTileA;
+        const float4 *co = reinterpret_cast<const float4 *>(bring + sb * bst + 2 * btile);
+        const int k0 = ks * kK;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        uint32_t h[4], l[4];
+        for (int q = 0; q < kKPerProducer / 4; ++q) {
+          uint32_t h[4], l[4];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int k = kbeg + q * 4 + e;
-          float g = 0.f;
-          if (gm < M_total && k0 + k < K_total) {
-            if (DIR == 0) g = PointKernel<float>::eval(own, own_n, co[k]);
-            else g = PointKernel<float>::eval(co[k], co[kK + k], own);
+          for (int e = 0; e < 4; ++e) {
+            const int k = kbeg + q * 4 + e;
+            float g = 0.f;
+            if (gm < M_total && k0 + k < K_total) {
+              if (DIR == 0) g = PointKernel<float>::eval(own, own_n, co[k]);
+              else g = PointKernel<float>::eval(co[k], co[kK + k], own);
+            }
+            split_tf32(g, h[e], l[e]);
           }
-          split_tf32(g, h[e], l[e]);
+          const uint32_t off = sw128(row, kbeg + q * 4);
+          *reinterpret_cast<uint4 *>(Ahi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+          *reinterpret_cast<uint4 *>(Alo + off) = make_uint4(l[0], l[1], l[2], l[3]);
         }
-        const uint32_t off = sw128(row, kbeg + q * 4);
-        *reinterpret_cast<uint4 *>(Ahi + off) = make_uint4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<uint4 *>(Alo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("bar.sync %0, %1;" ::"n"(kBarAReady), "n"(kGoCount) : "memory");
+    }
+  } else if (warp == kSchedWarp) {
+    // ---------------- scheduler: releases the producers step by step ----------------
+    for (int ks = 0; ks < nks; ++ks) {
+      if (lane == 0 && !*vfail) {
+        if (!mbar_wait_one(&bfull[ks % nbs], (ks / nbs) & 1) ||
+            !mbar_wait_one(&aempty[ks % kAStages], ((ks / kAStages) & 1) ^ 1))
+          *s_fail = 1;
+      }
       __syncwarp();
-      if (lane == 0) mbar_arrive(&a_full[s]);
+      asm volatile("bar.sync %0, %1;" ::"n"(kBarGo), "n"(kGoCount) : "memory");
     }
   } else if (warp == kLoaderWarp) {
     // ---------------- loader: coordinates + B image by bulk copy ----------------
@@ -382,55 +426,49 @@ __global__ void __launch_bounds__(kThreads, 1) pk_tc_kernel(TcArgs a)
       const uint32_t bbytes = 2 * btile;
       int issued = 0;
       for (int ks = 0; ks < nks; ++ks) {
-        const int s = ks % kStages;
-        if (!mbar_wait_one(&empty[s], ((ks / kStages) & 1) ^ 1)) {
+        const int sb = ks % nbs;
+        if (*vfail || !mbar_wait_one(&bempty[sb], ((ks / nbs) & 1) ^ 1, 32)) {
           *s_fail = 1;
           break;
         }
-        unsigned char *st = smem + s * sb;
-        unsigned char *bdst = st + 2 * kTileA;
+        unsigned char *bdst = bring + sb * bst;
         unsigned char *cdst = bdst + 2 * btile;
         const int k0 = ks * kK;
-        mbar_arrive_tx(&tma_full[s], cbytes + bbytes);
+        mbar_arrive_tx(&bfull[sb], cbytes + bbytes);
         bulk_g2s(bdst, reinterpret_cast<const unsigned char *>(a.bimg) + (size_t)ks * bbytes, bbytes,
-                 &tma_full[s]);
+                 &bfull[sb]);
         if (DIR == 0) {
-          bulk_g2s(cdst, a.ys + k0, cbytes, &tma_full[s]);
+          bulk_g2s(cdst, a.ys + k0, cbytes, &bfull[sb]);
         } else {
           // the 32 rows' points, then their normals
-          bulk_g2s(cdst, a.xr + k0, cbytes / 2, &tma_full[s]);
-          bulk_g2s(cdst + cbytes / 2, a.nr + k0, cbytes / 2, &tma_full[s]);
+          bulk_g2s(cdst, a.xr + k0, cbytes / 2, &bfull[sb]);
+          bulk_g2s(cdst + cbytes / 2, a.nr + k0, cbytes / 2, &bfull[sb]);
         }
         ++issued;
       }
       // no copy may still be landing when the CTA exits
-      for (int ks = issued > kStages ? issued - kStages : 0; ks < issued; ++ks)
-        if (!mbar_wait_one(&tma_full[ks % kStages], (ks / kStages) & 1)) *s_fail = 1;
+      for (int ks = issued > nbs ? issued - nbs : 0; ks < issued; ++ks)
+        if (!mbar_wait_one(&bfull[ks % nbs], (ks / nbs) & 1)) *s_fail = 1;
     }
   } else if (warp == kMmaWarp) {
     // ---------------- MMA issue ----------------
-    if (lane == 0) {
-      const uint32_t idesc = idesc_tf32(a.np);
-      bool broke = false;
-      for (int ks = 0; ks < nks; ++ks) {
-        const int s = ks % kStages;
-        const int kc = ks % kChunk;
-        // a new chunk overwrites the accumulator: the previous one must be folded
-        if (kc == 0 && ks > 0 && !mbar_wait_one(chunk_free, ((ks / kChunk) - 1) & 1)) {
+    const uint32_t idesc = idesc_tf32(a.np);
+    for (int ks = 0; ks < nks; ++ks) {
+      const int sa = ks % kAStages, sb = ks % nbs;
+      const int kc = ks % kChunk;
+      if (lane == 0 && !*vfail) {
+        // the B stage (normally landed long ago), and at a chunk start the
+        // previous chunk folded out of the accumulator
+        if (!mbar_wait_one(&bfull[sb], (ks / nbs) & 1) ||
+            (kc == 0 && ks > 0 && !mbar_wait_one(chunk_free, ((ks / kChunk) - 1) & 1)))
           *s_fail = 1;
-          broke = true;
-          break;
-        }
-        if (!mbar_wait_one(&a_full[s], (ks / kStages) & 1) ||
-            !mbar_wait_one(&tma_full[s], (ks / kStages) & 1)) {
-          *s_fail = 1;
-          broke = true;
-          break;
-        }
+      }
+      __syncwarp();
+      asm volatile("bar.sync %0, %1;" ::"n"(kBarAReady), "n"(kGoCount) : "memory");
+      if (lane == 0 && !*vfail) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t st = smem_u32(smem + s * sb);
-        const uint32_t Ahi = st, Alo = st + kTileA;
-        const uint32_t Bhi = st + 2 * kTileA, Blo = Bhi + btile;
+        const uint32_t Ahi = smem_u32(smem + sa * 2 * kTileA), Alo = Ahi + kTileA;
+        const uint32_t Bhi = smem_u32(bring + sb * bst), Blo = Bhi + btile;
 #pragma unroll
         for (int kk = 0; kk < kK / 8; ++kk) {
           const uint32_t ko = kk * 32;  // 8 TF32 = 32 bytes along the swizzled row
@@ -439,13 +477,16 @@ __global__ void __launch_bounds__(kThreads, 1) pk_tc_kernel(TcArgs a)
           mma_tf32(tmem_acc, desc_sw128(Ahi + ko), desc_sw128(Blo + ko), idesc, 1u);
           mma_tf32(tmem_acc, desc_sw128(Ahi + ko), desc_sw128(Bhi + ko), idesc, 1u);
         }
-        mma_commit(&empty[s]);
+        mma_commit(&aempty[sa]);
+        mma_commit(&bempty[sb]);
         if (kc == kChunk - 1 || ks == nks - 1) mma_commit(chunk_full);
       }
-      // after an early exit, release the accumulator warps once every MMA
-      // issued so far has finished
-      if (broke) mma_commit(chunk_full);
-      // tensor memory is freed only after every issued MMA has finished
+      __syncwarp();
+    }
+    if (lane == 0) {
+      // after a failure, release the accumulator warps once every MMA issued
+      // so far has finished; tensor memory is freed only after that point
+      if (*vfail) mma_commit(chunk_full);
       mma_commit(mma_done);
       if (!mbar_wait_one(mma_done, 0)) *s_fail = 1;
     }
@@ -456,7 +497,9 @@ __global__ void __launch_bounds__(kThreads, 1) pk_tc_kernel(TcArgs a)
     const uint32_t lane_off = (uint32_t)(q * 32) << 16;
     bool ok = true;
     for (int c = 0; c < nchunks; ++c) {
-      if (!mbar_wait_warp(chunk_full, c & 1)) {
+      if (warp == kAccWarp0 && lane == 0) s_aflag[c & 1] = mbar_wait_one(chunk_full, c & 1, 64) ? 1 : 0;
+      asm volatile("bar.sync %0, 128;" ::"n"(kBarAcc) : "memory");
+      if (!s_aflag[c & 1]) {
         ok = false;
         break;
       }
