@@ -215,3 +215,28 @@ class Solver:
         T = torch.empty((self.n, R), dtype=W.dtype, device=W.device)
         check(load().mbc_apply_KT(self._h, R, W.data_ptr(), T.data_ptr(), self._sp()), "mbc_apply_KT")
         return T[:, 0] if W.dim() == 1 else T
+
+    def added_mass(self, X, weights, body_ptr, centers, rho_fluid=1.0, accel=None):
+        """Added-mass tensor (6 bodies x R, FP64) of strengths X (n x R, original
+        order) and, given a generalized acceleration (R = 6 bodies), the fluid
+        forces -Mf a (mbc_added_mass).  weights: nf quadrature weights."""
+        import torch
+
+        X = X.contiguous()
+        if X.dim() == 1:
+            X = X[:, None]
+        R = X.shape[1]
+        w = torch.as_tensor(np.asarray(weights, np.float32), device=X.device).contiguous()
+        bp = np.ascontiguousarray(body_ptr, np.int32)
+        cen = np.ascontiguousarray(centers, np.float64)
+        nb = bp.shape[0] - 1
+        Mf = np.empty((6 * nb, R), np.float64)
+        acc = None if accel is None else np.ascontiguousarray(accel, np.float64)
+        frc = None if accel is None else np.empty(6 * nb, np.float64)
+        dt = MBC_F64 if X.dtype == torch.float64 else MBC_F32
+        check(load().mbc_added_mass(self._h, R, X.data_ptr(), dt, w.data_ptr(), nb, bp.ctypes.data,
+                                    cen.ctypes.data, float(rho_fluid), Mf.ctypes.data,
+                                    None if acc is None else acc.ctypes.data,
+                                    None if frc is None else frc.ctypes.data, self._sp()),
+              "mbc_added_mass")
+        return (Mf, frc) if accel is not None else Mf

@@ -85,6 +85,15 @@ SIGNATURES = {
                                     C.POINTER(SolveStats), _vp, _vp]),
     "mbc_apply_K": (C.c_int, [_vp, _i32, _vp, _vp, _vp]),
     "mbc_apply_KT": (C.c_int, [_vp, _i32, _vp, _vp, _vp]),
+    "mbc_added_mass": (C.c_int, [_vp, _i32, _vp, _i32, _vp, _i32, _vp, _vp, _d, _vp, _vp, _vp, _vp]),
+    "mbc_mlp_create": (C.c_int, [_i32, _i32, _i32, _i32, C.c_uint64, C.POINTER(_vp)]),
+    "mbc_mlp_destroy": (C.c_int, [_vp]),
+    "mbc_mlp_num_params": (C.c_int, [_vp, C.POINTER(_i64)]),
+    "mbc_mlp_get_params": (C.c_int, [_vp, _vp]),
+    "mbc_mlp_set_params": (C.c_int, [_vp, _vp]),
+    "mbc_mlp_forward": (C.c_int, [_vp, _i32, _vp, _vp, _vp]),
+    "mbc_mlp_train_step": (C.c_int, [_vp, _i32, _vp, _vp, C.c_float, _vp, _vp, _vp]),
+    "mbc_warm_correct": (C.c_int, [_i32, _i32, _vp, _i32, _vp, _vp, _vp, _vp]),
     "mbc_point_apply_noalloc": (C.c_int, [_i32, _i32, _i32, _vp, _vp, _vp, C.c_double, _i32, _vp, _vp, _vp]),
     "mbc_context_create": (C.c_int, [C.POINTER(_vp)]),
     "mbc_context_destroy": (C.c_int, [_vp]),

@@ -60,10 +60,21 @@ struct PointKernel<double> {
   }
 };
 
+// Single-layer potential kernel 1/|x - y| in FP64 (the normal is unused):
+// the potential of the solved strengths, utils/torch_utils.py:254-276.
+struct SingleLayer64 {
+  __device__ __forceinline__ static double eval(const float4 &x, const float4 &, const float4 &y)
+  {
+    const double dx = (double)x.x - (double)y.x, dy = (double)x.y - (double)y.y,
+                 dz = (double)x.z - (double)y.z;
+    return rsqrt_nr(fma(dz, dz, fma(dy, dy, dx * dx)));
+  }
+};
+
 // Rows direction.  Block = TI threads, one row each; grid.x over rows,
 // grid.y over RC-column chunks.  `done` (may be NULL) lets an iteration that
 // has nothing left to do exit at once.
-template <typename T, int RC, int TI, int TJ>
+template <typename T, int RC, int TI, int TJ, class Ker = PointKernel<T>>
 __global__ void __launch_bounds__(TI) pk_rows_kernel(
     const float4 *__restrict__ xr, const float4 *__restrict__ nr, int nf,
     const float4 *__restrict__ ys, int n, const T *__restrict__ v, int ldv,
@@ -95,13 +106,13 @@ __global__ void __launch_bounds__(TI) pk_rows_kernel(
     if (jm == TJ) {
 #pragma unroll 2
       for (int jj = 0; jj < TJ; ++jj) {
-        const T k = PointKernel<T>::eval(xi, ni, sy[jj]);
+        const T k = Ker::eval(xi, ni, sy[jj]);
 #pragma unroll
         for (int r = 0; r < RC; ++r) acc[r] = fma(k, sv[jj * RC + r], acc[r]);
       }
     } else {
       for (int jj = 0; jj < jm; ++jj) {
-        const T k = PointKernel<T>::eval(xi, ni, sy[jj]);
+        const T k = Ker::eval(xi, ni, sy[jj]);
 #pragma unroll
         for (int r = 0; r < RC; ++r) acc[r] = fma(k, sv[jj * RC + r], acc[r]);
       }
@@ -289,3 +300,4 @@ __global__ void __launch_bounds__(TI) dense_cols_kernel(
 }
 
 }  // namespace mbc
+

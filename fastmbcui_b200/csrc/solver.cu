@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include "factor.cuh"
+#include "forces.cuh"
 #include "matvec.cuh"
 #include "matvec_tc.cuh"
 #include "mbc_internal.h"
@@ -230,6 +231,8 @@ int launch_cols(const Solver &S, int R, const T *w, T *t, const T *pdot, double 
   return cols_launch<T, 32, 64>(S, R, w, t, pdot, part, done, st);
 }
 
+// upper bound on the blocks of any columns-direction launch (the per-block
+// curvature partials): SIMT tiles of 64 sources or more, tensor cores 128
 int cols_blocks(const Solver &S) { return (int)cdiv(S.n, 64); }
 
 template void launch_rows<float>(const Solver &, int, const float *, float *, const int32_t *, cudaStream_t);
@@ -1272,5 +1275,61 @@ extern "C" mbc_status mbc_apply_KT(mbc_solver *s, int32_t R, const void *W, void
     mbc::permute_out<float>(S, R, (const float *)S.tmp.ptr, T, MBC_F32, st);
   }
   MBC_CKL();
+  return S.check_device_error(st);
+}
+
+// Added-mass tensor and fluid forces from solved strengths (see mbc.h).
+extern "C" mbc_status mbc_added_mass(mbc_solver *s, int32_t R, const void *X, int32_t x_dtype, const float *w,
+                                     int32_t n_bodies, const int32_t *body_ptr, const double *centers,
+                                     double rho_fluid, double *Mf, const double *accel, double *forces,
+                                     mbc_stream stream)
+{
+  if (!s || R <= 0 || !X || !w || n_bodies <= 0 || !body_ptr || !centers || !Mf)
+    return fail(MBC_BAD_ARG, "mbc_added_mass: NULL pointer or non-positive size");
+  if (x_dtype != MBC_F32 && x_dtype != MBC_F64) return fail(MBC_BAD_ARG, "mbc_added_mass: bad x_dtype");
+  if ((accel == nullptr) != (forces == nullptr))
+    return fail(MBC_BAD_ARG, "mbc_added_mass: accel and forces go together");
+  if (accel && R != 6 * n_bodies)
+    return fail(MBC_BAD_ARG, "mbc_added_mass: forces need R == 6 * n_bodies (all rigid modes)");
+  mbc::Solver &S = s->s;
+  if (S.op.kind != MBC_OP_POINT_KERNEL)
+    return fail(MBC_UNSUPPORTED, "mbc_added_mass: needs a point-kernel operator (source positions)");
+  if (body_ptr[0] != 0) return fail(MBC_BAD_ARG, "mbc_added_mass: body_ptr[0] must be 0");
+  for (int a = 0; a < n_bodies; ++a)
+    if (body_ptr[a + 1] < body_ptr[a] || body_ptr[a + 1] > S.nf)
+      return fail(MBC_BAD_ARG, "mbc_added_mass: body_ptr must ascend within [0, nf]");
+  if ((R + 31) / 32 > 65535) return fail(MBC_BAD_ARG, "mbc_added_mass: R too large");
+  cudaStream_t st = (cudaStream_t)stream;
+  mbc::DevMem xp, phi, dmf, dptr, dcen;
+  MBC_TRY(xp.reserve(sizeof(double) * (size_t)S.n * R));
+  MBC_TRY(phi.reserve(sizeof(double) * (size_t)S.nf * R));
+  MBC_TRY(dmf.reserve(sizeof(double) * (size_t)6 * n_bodies * R));
+  MBC_TRY(dptr.reserve(sizeof(int32_t) * (size_t)(n_bodies + 1)));
+  MBC_TRY(dcen.reserve(sizeof(double) * (size_t)3 * n_bodies));
+  MBC_CK(cudaMemcpyAsync(dptr.ptr, body_ptr, sizeof(int32_t) * (n_bodies + 1), cudaMemcpyHostToDevice, st));
+  MBC_CK(cudaMemcpyAsync(dcen.ptr, centers, sizeof(double) * 3 * n_bodies, cudaMemcpyHostToDevice, st));
+  // phi = SL X in FP64 (strengths gathered into the plan order of the sources)
+  mbc::permute_in<double>(S, R, X, x_dtype, (double *)xp.ptr, st);
+  {
+    constexpr int RC = 16, TI = 64;
+    dim3 grid(mbc::cdiv(S.nf, TI), mbc::cdiv(R, RC));
+    mbc::pk_rows_kernel<double, RC, TI, mbc::TJ_ROWS, mbc::SingleLayer64><<<grid, TI, 0, st>>>(
+        S.x4(), S.n4(), S.nf, S.y4(), S.n, (const double *)xp.ptr, R, 1.0 / (4.0 * 3.14159265358979323846),
+        (double *)phi.ptr, R, R, nullptr);
+  }
+  mbc::added_mass_kernel<<<dim3(n_bodies, mbc::cdiv(R, 32)), 256, 0, st>>>(
+      S.x4(), S.n4(), w, (const int32_t *)dptr.ptr, (const double *)dcen.ptr, (const double *)phi.ptr, R,
+      rho_fluid, (double *)dmf.ptr);
+  MBC_CKL();
+  MBC_CK(cudaMemcpyAsync(Mf, dmf.ptr, sizeof(double) * (size_t)6 * n_bodies * R, cudaMemcpyDeviceToHost, st));
+  MBC_CK(cudaStreamSynchronize(st));
+  if (accel) {
+    // reactive force of the added mass: f = -Mf a
+    for (int i = 0; i < 6 * n_bodies; ++i) {
+      double f = 0.0;
+      for (int j = 0; j < R; ++j) f += Mf[(size_t)i * R + j] * accel[j];
+      forces[i] = -f;
+    }
+  }
   return S.check_device_error(st);
 }

@@ -71,6 +71,23 @@ class Scene:
             f[rows, 6 * b + 3:6 * b + 6] = np.cross(r, n)
         return _f32(f)
 
+    def body_ptr(self) -> np.ndarray:
+        """Row offsets of the bodies (rows of body b are [ptr[b], ptr[b+1]))."""
+        ptr = np.searchsorted(self.row_body, np.arange(self.n_bodies + 1)).astype(np.int32)
+        if not np.array_equal(np.repeat(np.arange(self.n_bodies), np.diff(ptr)), self.row_body):
+            raise ValueError("rows are not grouped by body")
+        return ptr
+
+    def weights(self) -> np.ndarray:
+        """Quadrature weight of each collocation point: its body's area over
+        its point count (the points are area-uniform samples)."""
+        if "weights" in self.meta:
+            return _f32(np.asarray(self.meta["weights"], dtype=np.float64))
+        ptr = self.body_ptr()
+        areas = np.asarray(self.meta["areas"], dtype=np.float64)
+        w = np.repeat(areas / np.diff(ptr), np.diff(ptr))
+        return _f32(w)
+
     def dense_K(self) -> np.ndarray:
         """Dense FP64 operator (nf x n); only for small scenes."""
         r = self.x[:, None, :] - self.y[None, :, :]
@@ -151,6 +168,17 @@ def sample_ellipsoid(rng: np.random.Generator, npts: int, axes):
     return p, n
 
 
+def ellipsoid_area(axes, n_theta: int = 2000) -> float:
+    """Surface area of an ellipsoid by the midpoint rule in (theta, phi)."""
+    a, b, c = (float(v) for v in axes)
+    th = (np.arange(n_theta) + 0.5) * np.pi / n_theta
+    ph = (np.arange(2 * n_theta) + 0.5) * np.pi / n_theta
+    st, ct = np.sin(th)[:, None], np.cos(th)[:, None]
+    sp, cp = np.sin(ph)[None, :], np.cos(ph)[None, :]
+    g = st * np.sqrt((b * c * st * cp) ** 2 + (a * c * st * sp) ** 2 + (a * b * ct) ** 2)
+    return float(g.sum() * (np.pi / n_theta) ** 2)
+
+
 def sample_box(rng: np.random.Generator, npts: int, side: float):
     """Area-uniform points on a cube of edge ``side``; (p, n)."""
     face = rng.integers(0, 6, npts)
@@ -217,7 +245,7 @@ def sphere_scene(subdiv: int = 4, src_radius: float = 0.8) -> Scene:
     """
     v = icosphere(subdiv)
     return _assemble(f"sphere_ico{subdiv}", [(v, v, src_radius * v, np.zeros(3))],
-                     rho=3.0, lam=1.5, tol=1e-10)
+                     rho=3.0, lam=1.5, tol=1e-10, meta={"areas": [4 * np.pi]})
 
 
 def coins_scene(n_coins: int = 16, pts: int = 4000, offset: float = 0.02,
@@ -240,7 +268,8 @@ def coins_scene(n_coins: int = 16, pts: int = 4000, offset: float = 0.02,
         R = random_rotation(rp)
         p, n = p @ R.T + centers[b], n @ R.T
         parts.append((p, n, p - offset * n, centers[b]))
-    return _assemble(f"coins{n_coins}x{pts}", parts, rho=3.0, lam=1.5, tol=1e-8)
+    return _assemble(f"coins{n_coins}x{pts}", parts, rho=3.0, lam=1.5, tol=1e-8,
+                     meta={"areas": [2 * np.pi * 0.1 + 2 * np.pi] * n_coins})
 
 
 def ellipsoids_scene(n_bodies: int, pts, seed: int, box: float = 10.0,
@@ -262,7 +291,36 @@ def ellipsoids_scene(n_bodies: int, pts, seed: int, box: float = 10.0,
         p, n = p @ R.T, n @ R.T
         parts.append((p + centers[b], n, p - offset * n + centers[b], centers[b]))
     return _assemble(f"ellipsoids{n_bodies}", parts, rho=3.0, lam=1.5, tol=1e-8,
-                     meta={"axes": axes})
+                     meta={"axes": axes, "areas": [ellipsoid_area(ax) for ax in axes]})
+
+
+def fibonacci_sphere(npts: int) -> np.ndarray:
+    """Quasi-uniform unit vectors (Fibonacci lattice), equal area 4 pi / npts each."""
+    i = np.arange(npts) + 0.5
+    z = 1.0 - 2.0 * i / npts
+    th = np.pi * (1.0 + 5.0 ** 0.5) * i
+    r = np.sqrt(1.0 - z * z)
+    return np.stack([r * np.cos(th), r * np.sin(th), z], 1)
+
+
+def ellipsoid_fibonacci_scene(axes, npts: int = 2000, offset: float = 0.15) -> Scene:
+    """One ellipsoid at the origin (principal axes along x, y, z) sampled on the
+    mapped Fibonacci lattice, with exact quadrature weights
+    (4 pi / npts) abc |A^-T u|; sources `offset` inside along the normal.
+
+    A smooth quadrature with the sources more than a point spacing inside:
+    its added mass matches Lamb's closed form to ~1e-5 (with random
+    area-uniform points and sources closer than the spacing the potential
+    between the points is poor and the added mass is off by ~10 %).
+    """
+    A = np.asarray(axes, dtype=np.float64)
+    u = fibonacci_sphere(npts)
+    p = u * A
+    n = p / (A * A)
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    w = (4.0 * np.pi / npts) * np.prod(A) * np.linalg.norm(u / A, axis=1)
+    return _assemble(f"ellipsoid_fib{npts}", [(p, n, p - offset * n, np.zeros(3))], rho=3.0, lam=1.5,
+                     tol=1e-10, meta={"axes": A[None], "areas": [ellipsoid_area(A)], "weights": w})
 
 
 def uneven_batch(n_scenes: int = 256, first_seed: int = 3):
@@ -276,10 +334,10 @@ def uneven_batch(n_scenes: int = 256, first_seed: int = 3):
     return out
 
 
-def trajectory_poses(n_bodies: int, steps: int, seed: int, dt: float = 0.01):
+def trajectory_poses(n_bodies: int, steps: int, seed: int, dt: float = 0.01, amp_range=(0.05, 0.3)):
     """Smooth rigid motions: each of the 6 DOF of a body is a sum of 4 sinusoids."""
     rng = np.random.default_rng(seed)
-    amp = rng.uniform(0.05, 0.3, size=(n_bodies, 6, 4))
+    amp = rng.uniform(amp_range[0], amp_range[1], size=(n_bodies, 6, 4))
     freq = rng.uniform(0.2, 2.0, size=(n_bodies, 6, 4))
     phase = rng.uniform(0, 2 * np.pi, size=(n_bodies, 6, 4))
     t = np.arange(steps) * dt
@@ -287,3 +345,73 @@ def trajectory_poses(n_bodies: int, steps: int, seed: int, dt: float = 0.01):
     v = (amp[None] * 2 * np.pi * freq[None] *
          np.cos(2 * np.pi * freq[None] * t[:, None, None, None] + phase[None])).sum(-1)
     return q, v  # steps x bodies x 6 (translation, rotation vector)
+
+
+def rotvec_matrix(v) -> np.ndarray:
+    """Rotation matrix of a rotation vector (Rodrigues)."""
+    v = np.asarray(v, dtype=np.float64)
+    th = float(np.linalg.norm(v))
+    if th < 1e-300:
+        return np.eye(3)
+    k = v / th
+    K = np.array([[0.0, -k[2], k[1]], [k[2], 0.0, -k[0]], [-k[1], k[0], 0.0]])
+    return np.eye(3) + np.sin(th) * K + (1.0 - np.cos(th)) * (K @ K)
+
+
+def moved(sc: Scene, q) -> Scene:
+    """The scene with body b displaced by q[b] = (translation, rotation vector)
+    about its centre; points keep their indices (rows, sources, bodies)."""
+    q = np.asarray(q, dtype=np.float64)
+    x = sc.x.astype(np.float64).copy()
+    nx = sc.nx.astype(np.float64).copy()
+    y = sc.y.astype(np.float64).copy()
+    cen = sc.centers.astype(np.float64).copy()
+    for b in range(sc.n_bodies):
+        R = rotvec_matrix(q[b, 3:6])
+        c = cen[b]
+        rows = sc.row_body == b
+        srcs = sc.src_body == b
+        x[rows] = (x[rows] - c) @ R.T + c + q[b, :3]
+        nx[rows] = nx[rows] @ R.T
+        y[srcs] = (y[srcs] - c) @ R.T + c + q[b, :3]
+        cen[b] = c + q[b, :3]
+    nx /= np.linalg.norm(nx, axis=1, keepdims=True)
+    meta = dict(sc.meta)
+    meta["pose"] = q
+    return Scene(name=sc.name, x=_f32(x), nx=_f32(nx), y=_f32(y), row_body=sc.row_body,
+                 src_body=sc.src_body, centers=_f32(cen), coef=sc.coef, rho=sc.rho, lam=sc.lam,
+                 max_super=sc.max_super, tol=sc.tol, meta=meta)
+
+
+def trajectory_scene(n_bodies: int = 32, pts: int = 2000, seed: int = 4, steps: int = 500,
+                     dt: float = 0.01, amp_range=(0.005, 0.03), box: float = 12.0):
+    """The 32-ellipsoid trajectory: a base scene whose bodies are placed with
+    room for their motion, and the poses (steps x bodies x 6) and velocities.
+
+    Each DOF is a sum of 4 seeded sinusoids; with amplitudes U(0.005, 0.03)
+    a body moves at most 0.12 per axis and turns at most 0.12 rad, and the
+    placement margin keeps the bodies apart along the whole trajectory (which
+    needs a 12^3 box for 32 bodies).
+    """
+    rng = np.random.default_rng(seed)
+    axes = rng.uniform(0.5, 1.5, size=(n_bodies, 3))
+    # a bounding sphere about the centre only translates (by <= sqrt(3) * 4 amp)
+    radii = axes.max(axis=1) + np.sqrt(3.0) * 4 * amp_range[1]
+    while True:  # grow the box until the seeded placement succeeds
+        try:
+            centers = random_centers(rng, radii, box)
+            break
+        except RuntimeError:
+            box += 0.5
+    parts, rots = [], []
+    for b in range(n_bodies):
+        p, n = sample_ellipsoid(rng, pts, axes[b])
+        R = random_rotation(rng)
+        rots.append(R)
+        p, n = p @ R.T, n @ R.T
+        parts.append((p + centers[b], n, p - 0.05 * n + centers[b], centers[b]))
+    base = _assemble(f"trajectory{n_bodies}", parts, rho=3.0, lam=1.5, tol=1e-8,
+                     meta={"axes": axes, "areas": [ellipsoid_area(ax) for ax in axes],
+                           "rot": np.array(rots)})
+    q, v = trajectory_poses(n_bodies, steps, seed + 1, dt, amp_range)
+    return base, q, v

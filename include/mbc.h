@@ -198,6 +198,58 @@ mbc_status mbc_solve_adjoint(mbc_solver *s, int32_t R, const void *B, int32_t b_
 mbc_status mbc_apply_K(mbc_solver *s, int32_t R, const void *V, void *W, mbc_stream stream);
 mbc_status mbc_apply_KT(mbc_solver *s, int32_t R, const void *W, void *T, mbc_stream stream);
 
+/* Added-mass tensor and fluid forces of solved strengths: the consumer of the
+ * solve in core/KTAB_Mfs_spclf1d.py:123-128 (phi = SL @ strengths,
+ * Ks = Q @ phi * rho_fluid), with compute_single_layer and compute_quadrature
+ * of utils/torch_utils.py:254-276, :336-347.  Point-kernel solvers only:
+ *   phi(x_i, c) = sum_j X[j, c] / (4 pi |x_i - y_j|)               (FP64)
+ *   Mf[6a + m, c] = -rho_fluid sum_{i in body a} w_i N_m(i) phi(x_i, c),
+ *   N = (n, (x - centre_a) x n)   (the rigid-mode order of the right-hand sides).
+ * The reference's SL is 1/|x - y| next to its solid-angle operator; with the
+ * normal derivative of G = 1/(4 pi r) the same potential carries 1/(4 pi).
+ * X: device n x R (x_dtype, ORIGINAL order); w: device nf float32 quadrature
+ * weights; body_ptr: host int32[n_bodies + 1], rows of body a are
+ * [body_ptr[a], body_ptr[a+1]); centers: host n_bodies x 3; Mf: host
+ * (6 n_bodies) x R.  With accel (host double[R], R == 6 n_bodies) also
+ * forces[6 n_bodies] = -Mf accel.  Synchronises the stream. */
+mbc_status mbc_added_mass(mbc_solver *s, int32_t R, const void *X, int32_t x_dtype, const float *w,
+                          int32_t n_bodies, const int32_t *body_ptr, const double *centers,
+                          double rho_fluid, double *Mf, const double *accel, double *forces,
+                          mbc_stream stream);
+
+/* ------------------------------------------------------------------------ */
+/* Warm-start network: a small MLP trained and evaluated on the GPU by this  */
+/* library's own kernels.  No counterpart in the reference (its PCG always   */
+/* starts from x0 = 0, kl_chol.cu:930-940): the network predicts a warm      */
+/* start that the PCG then refines, with the FP64 true residual as judge.     */
+/* Layers n_in -> hidden (tanh) x n_hidden_layers -> n_out (linear); BF16     */
+/* weights in the products, FP32 accumulation, FP32 master weights + Adam.   */
+/* Parameter vector layout: per layer W (row-major out x in), then b.        */
+/* X, Y, T: device row-major batch x n_in / batch x n_out float32.          */
+/* ------------------------------------------------------------------------ */
+typedef struct mbc_mlp mbc_mlp;
+mbc_status mbc_mlp_create(int32_t n_in, int32_t hidden, int32_t n_hidden_layers, int32_t n_out,
+                          uint64_t seed, mbc_mlp **out);
+mbc_status mbc_mlp_destroy(mbc_mlp *net);
+mbc_status mbc_mlp_num_params(const mbc_mlp *net, int64_t *count);
+mbc_status mbc_mlp_get_params(const mbc_mlp *net, float *params_host);
+mbc_status mbc_mlp_set_params(mbc_mlp *net, const float *params_host);
+mbc_status mbc_mlp_forward(mbc_mlp *net, int32_t batch, const float *X, float *Y, mbc_stream stream);
+/* One step on the loss 0.5 mean((Y - T)^2): forward, backward and, for
+ * lr > 0, an Adam update.  loss_host / grads_host (optional, host) receive
+ * the batch loss and the gradient before the update. */
+mbc_status mbc_mlp_train_step(mbc_mlp *net, int32_t batch, const float *X, const float *T, float lr,
+                              double *loss_host, float *grads_host, mbc_stream stream);
+
+/* Warm-start correction in the basis of the isolated-body solutions:
+ *   X[j, 6b + m] += sum_k U[j, k] H[src_body[j]][b][k][m]
+ * U: device n x 6 (each body's own rigid-mode solution on its sources),
+ * H: device n_bodies x n_bodies x 6 x 6, X: device n x R float32 (ORIGINAL
+ * order, R <= 6 n_bodies), src_body: device int32[n].  No counterpart in the
+ * reference. */
+mbc_status mbc_warm_correct(int32_t n, int32_t R, const int32_t *src_body, int32_t n_bodies,
+                            const float *U, const float *H, float *X, mbc_stream stream);
+
 /* Point-kernel matvec that allocates no device memory.  No counterpart in the
  * reference: it serves callers that cannot let a library call cudaMalloc or
  * cudaFree -- hosts that own the device through their own memory pool or a

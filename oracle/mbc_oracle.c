@@ -629,6 +629,55 @@ int orc_pcg(int nf, int n, const double *M, const double *x, const double *nx,
   return it;
 }
 
+/*
+ * Added-mass tensor of a solved scene (the parity observable downstream of
+ * the solve): core/KTAB_Mfs_spclf1d.py:123-128 with utils/torch_utils.py
+ * compute_single_layer (:254-276) and compute_quadrature (:336-347).
+ *   phi = SL X,  SL(i, j) = 1 / (4 pi |x_i - y_j|)
+ *   Mf[6a + m, c] = -rho_f sum_{k in body a} w_k N_m(k) phi(k, c),
+ *   N(k) = (n_k, (x_k - centre_a) x n_k).
+ * The reference pairs its solid-angle operator with SL = 1/|x - y|; with the
+ * normal-derivative operator of G = 1/(4 pi r) used here the same potential
+ * carries the 1/(4 pi).  X: n x R row-major (original source order); w: nf
+ * quadrature weights; body_ptr: rows of body a are [body_ptr[a], body_ptr[a+1]).
+ */
+void orc_added_mass(int nf, int n, const double *x, const double *nx, const double *y, int R,
+                    const double *X, const double *w, int nb, const int32_t *body_ptr,
+                    const double *centers, double rho_f, double *Mf)
+{
+  double *phi = (double *)malloc(sizeof(double) * (size_t)nf * R);
+  int i;
+#pragma omp parallel for schedule(static)
+  for (i = 0; i < nf; ++i) {
+    double *pr = phi + (size_t)i * R;
+    int j, c;
+    for (c = 0; c < R; ++c) pr[c] = 0.0;
+    for (j = 0; j < n; ++j) {
+      const double g = 1.0 / (4.0 * 3.14159265358979323846 * sqrt(sq3(&x[3 * i], &y[3 * j])));
+      const double *xr = X + (size_t)j * R;
+      for (c = 0; c < R; ++c) pr[c] += g * xr[c];
+    }
+  }
+  int a;
+  for (a = 0; a < nb; ++a) {
+    int m, c, k;
+    for (m = 0; m < 6; ++m)
+      for (c = 0; c < R; ++c) Mf[(size_t)(6 * a + m) * R + c] = 0.0;
+    for (k = body_ptr[a]; k < body_ptr[a + 1]; ++k) {
+      const double *nk = &nx[3 * k];
+      const double r0 = x[3 * k] - centers[3 * a], r1 = x[3 * k + 1] - centers[3 * a + 1],
+                   r2 = x[3 * k + 2] - centers[3 * a + 2];
+      const double N[6] = {nk[0], nk[1], nk[2], r1 * nk[2] - r2 * nk[1], r2 * nk[0] - r0 * nk[2],
+                           r0 * nk[1] - r1 * nk[0]};
+      for (m = 0; m < 6; ++m)
+        for (c = 0; c < R; ++c) Mf[(size_t)(6 * a + m) * R + c] += w[k] * N[m] * phi[(size_t)k * R + c];
+    }
+    for (m = 0; m < 6; ++m)
+      for (c = 0; c < R; ++c) Mf[(size_t)(6 * a + m) * R + c] *= -rho_f;
+  }
+  free(phi);
+}
+
 int orc_num_threads(void)
 {
 #ifdef _OPENMP

@@ -56,6 +56,9 @@ def lib():
         L.orc_factor.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, C.c_double, _i32p, C.c_int,
                                  _i32p, _i32p, _i32p, _i32p, _i64p, _f64p, _i32p, _i32p, _f64p,
                                  C.POINTER(C.c_int32)]
+        L.orc_added_mass.argtypes = [C.c_int, C.c_int, _f64p, _f64p, _f64p, C.c_int, _f64p, _f64p, C.c_int,
+                                     _i32p, _f64p, C.c_double, _f64p]
+        L.orc_added_mass.restype = None
         L.orc_precond.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, _f64p]
         L.orc_pcg.restype = C.c_int
         L.orc_pcg.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, C.c_double, _i32p, _i32p, _i32p,
@@ -271,6 +274,19 @@ def solve(op: Op, pl: dict, lval, F, maxits=1000, tol=1e-8):
         X[:, r] = xn[pl["P"]]
         its.append(it)
     return X, its
+
+
+def added_mass(sc, X, rho_f=1.0):
+    """Added-mass tensor (6 bodies x R) of strengths X (n x R, original order)
+    for a scene with area weights; FP64 (orc_added_mass)."""
+    X = np.ascontiguousarray(np.atleast_2d(np.asarray(X, np.float64).T).T)
+    R = X.shape[1]
+    nb = sc.n_bodies
+    out = np.empty((6 * nb, R))
+    f = lambda a: np.ascontiguousarray(a, np.float64)
+    lib().orc_added_mass(sc.nf, sc.n, f(sc.x), f(sc.nx), f(sc.y), R, X, f(sc.weights()), nb,
+                         np.ascontiguousarray(sc.body_ptr(), np.int32), f(sc.centers), float(rho_f), out)
+    return out
 
 
 def num_threads() -> int:

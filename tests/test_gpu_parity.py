@@ -66,7 +66,7 @@ def rel(a, b):
 
 
 @pytest.mark.parametrize("prec,tol", [(F.MBC_F64, 1e-12), (F.MBC_F32, 2e-5)])
-@pytest.mark.parametrize("R", [1, 3, 8, 40, 96])
+@pytest.mark.parametrize("R", [1, 3, 8, 40, 96, 97, 192, 250])
 def test_point_kernel_matvec(sphere, prec, tol, R):
     s = sphere.solver(prec)
     dt = torch.float64 if prec == F.MBC_F64 else torch.float32
@@ -305,3 +305,18 @@ def test_max_iters_reports_not_converged(ells):
     assert e.value.status == 1
     X, st, its = s.solve(_dev(Fm, torch.float64), iters=True, tol=1e-14, max_iters=5)
     assert its[0] == 5
+
+
+def test_fp64_batched_many_columns_matches_per_rhs():
+    # 30 columns: the batched FP64 path runs the GEMM-tiled matvec (with the
+    # fused curvature partials), the per-RHS path the one-column kernels
+    c = Case(S.ellipsoids_scene(5, 600, seed=3))
+    Fm = c.sc.rhs()
+    s = c.solver(F.MBC_F64)
+    Xb, stb, itb = s.solve(_dev(Fm, torch.float64), tol=1e-8, max_iters=3000, iters=True)
+    Xp, stp, itp = s.solve(_dev(Fm, torch.float64), tol=1e-8, max_iters=3000, iters=True,
+                           schedule=F.MBC_SCHED_PER_RHS)
+    assert stb["n_converged"] == Fm.shape[1] and stp["n_converged"] == Fm.shape[1]
+    fb, fp = c.op.K(Xb.cpu().numpy()), c.op.K(Xp.cpu().numpy())
+    assert np.linalg.norm(fb - fp) / np.linalg.norm(Fm) < 1e-6
+    assert np.all(np.abs(np.asarray(itb) - np.asarray(itp)) <= np.maximum(3, 0.03 * np.asarray(itp)))
