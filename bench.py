@@ -32,6 +32,7 @@ METRIC = "MFS solves/s at rel-res 1e-8 on 1 B200: mixed+batched+learned vs plain
 
 WORKLOADS = {
     # name: (builder, description)
+    "trajectory32": (None, "32 ellipsoids x 2000 points on a 500-step trajectory, N=Nf=64000, R=192"),
     "ellipsoids32": (lambda seed: _ell(32, 2000, seed), "32 ellipsoids x 2000 points, N=Nf=64000, R=192"),
     "ellipsoids8": (lambda seed: _ell(8, 2000, seed), "8 ellipsoids x 2000 points, N=Nf=16000, R=48"),
     "coins16": (lambda seed: _coins(seed), "16 coins x 4000 points, N=Nf=64000, R=96"),
@@ -55,6 +56,16 @@ def _sphere():
     from fastmbcui_b200 import scenes as S
 
     return S.sphere_scene()
+
+
+def _scene_for(name, seed):
+    """The scene a workload solves (the trajectory's at its first pose)."""
+    if name == "trajectory32":
+        from fastmbcui_b200 import scenes as S
+
+        base, q, _ = S.trajectory_scene(32, 2000, seed=seed, steps=500)
+        return S.moved(base, q[0])
+    return WORKLOADS[name][0](seed)
 
 
 def _peaks():
@@ -133,6 +144,181 @@ def _max_over_ranks(dist, v: float) -> float:
     t = torch.tensor([v], dtype=torch.float64, device="cuda")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def run_trajectory(args):
+    """The 32-ellipsoid trajectory: one step = the bodies move, a new factor,
+    and the mixed batched PCG of all 192 columns warm-started from the
+    previous step's strengths (the plan of each step is host work, reported as
+    its own column)."""
+    import torch
+
+    import fastmbcui_b200 as F
+    from fastmbcui_b200 import scenes as S
+
+    dist, rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    base, q, _ = S.trajectory_scene(32, 2000, seed=4 + rank, steps=500)
+    nsteps = args.warmup + args.steps
+    t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
+    scenes = [S.moved(base, q[k]) for k in range(nsteps + 1)]
+    t0 = time.perf_counter()
+    plans = [F.Plan(sc.y, sc.rho, sc.lam, sc.max_super) for sc in scenes]
+    t_plan = (time.perf_counter() - t0) / len(scenes)
+    coords = [(t(sc.x), t(sc.nx), t(sc.y)) for sc in scenes]  # inputs resident in HBM
+    Fm = [t(sc.rhs()) for sc in scenes]
+    R = Fm[0].shape[1]
+    opts = dict(tol=1e-8, max_iters=args.max_iters, max_refine=64, inner_tol=1e-2, check_every=8)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    # learned warm start: the trained network and the bodies' isolated
+    # solutions (a per-shape cache computed once, outside the timed steps)
+    ws = None
+    if args.warm == "learned":
+        from fastmbcui_b200 import warmstart as W
+
+        ws = W.WarmStart.load(args.warm_model)
+        U = W.isolated_basis(base)
+        sb = torch.as_tensor(base.src_body, dtype=torch.int32, device=dev)
+
+    def start(k, X_prev):
+        if X_prev is None or args.warm == "cold":
+            return None
+        if ws is None:
+            return X_prev
+        pairs = W.neighbour_pairs(scenes[k].centers)
+        f = W.pair_features(pairs, q[k - 1], q[k], base.centers, base.meta["axes"], base.meta["rot"])
+        return ws.apply(X_prev, U, sb, base.n_bodies, pairs, f)
+
+    def step(k, X_prev, profile=0):
+        x, nx, y = coords[k]
+        X0 = start(k, X_prev)
+        s = F.Solver(plans[k], x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F32)
+        s.set_matvec(MATVEC[args.matvec]).factor()
+        X, st = s.solve(Fm[k], X0=X0, out_dtype=torch.float32, profile=profile, **opts)
+        return X, st
+
+    X = None
+    cold = None
+    for k in range(args.warmup):
+        X, st = step(k, X)
+        if k == 0:
+            cold = st
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times, stats = [], []
+    with ClockSampler(local) as clk:
+        for k in range(args.warmup, nsteps):
+            flush.fill_(float(k))
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            ev0.record()
+            X, st = step(k, X, profile=1)
+            ev1.record()
+            torch.cuda.synchronize()
+            times.append(ev0.elapsed_time(ev1))
+            stats.append(st)
+    ms_step = _max_over_ranks(dist, float(np.mean(times)))
+    value = world * 1000.0 / ms_step
+
+    # end to end through the public API: host coordinates and the previous
+    # step's host strengths in, host strengths out, the host plan included
+    k = nsteps
+    sc = scenes[k]
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory()
+    hx, hnx, hy, hF, hX0 = pin(sc.x), pin(sc.nx), pin(sc.y), pin(sc.rhs()), pin(X.cpu().numpy())
+    hX = torch.empty((sc.n, R), dtype=torch.float32).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    dx, dnx, dy, dF, dX0 = (a.to(dev, non_blocking=True) for a in (hx, hnx, hy, hF, hX0))
+    pl2 = F.Plan(sc.y.astype(np.float64), sc.rho, sc.lam, sc.max_super)
+    s2 = F.Solver(pl2, x=dx, nx=dnx, y=dy, coef=sc.coef, precision=F.MBC_F32)
+    s2.set_matvec(MATVEC[args.matvec]).factor()
+    X2, _ = s2.solve(dF, X0=start(k, dX0), out_dtype=torch.float32, **opts)
+    hX.copy_(X2)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1000
+    e2e = world * 1000.0 / _max_over_ranks(dist, e2e_ms)
+    h2d = sum(a.numel() * 4 for a in (hx, hnx, hy, hF, hX0))
+    d2h = hX.numel() * 4
+    del s2, pl2
+
+    # plain FP64 GPU path on the first timed step: one cold-started PCG per
+    # column, a bounded sample of columns extrapolated to all R
+    k = args.warmup
+    x, nx, y = coords[k]
+    plain = F.Solver(plans[k], x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64)
+    ncol = min(R, args.plain_cols)
+    cols = np.linspace(0, R - 1, ncol).astype(int)
+    torch.cuda.synchronize()
+    ev0.record()
+    plain.factor()
+    ev1.record()
+    torch.cuda.synchronize()
+    t_fac64 = ev0.elapsed_time(ev1)
+    ev0.record()
+    Xp, stp = plain.solve(Fm[k][:, cols].double().contiguous(), tol=1e-8, max_iters=args.max_iters,
+                          schedule=F.MBC_SCHED_PER_RHS, check_every=8)
+    ev1.record()
+    torch.cuda.synchronize()
+    t_cols = ev0.elapsed_time(ev1)
+    plain_ms = t_fac64 + t_cols * R / ncol
+    plain_sps = 1000.0 / _max_over_ranks(dist, plain_ms)
+    del plain
+
+    st = stats[-1]
+    roofline = _matvec_roofline(st, scenes[0].nf, scenes[0].n, R, args.matvec)
+    out = {
+        "metric": METRIC, "value": round(value, 5), "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded trajectory)",
+        "config": {"workload": "trajectory32", "desc": WORKLOADS["trajectory32"][1], "N": base.n,
+                   "Nf": base.nf, "R": R, "rho": base.rho, "lambda": base.lam, "tol": 1e-8,
+                   "precision": "mixed FP32/FP64 residual replacement", "schedule": "batched",
+                   "warm_start": {"learned": "previous step + MLP correction (3x256, BF16 weights)",
+                                  "previous": "previous step's strengths", "cold": "x0 = 0"}[args.warm],
+                   "steps_run": f"{args.warmup} warm-up + {args.steps} timed",
+                   "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas{world}"},
+        "e2e": {"value": round(e2e, 5), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h),
+                "includes": "H2D of points, rhs and previous strengths; host plan; factor; solve; D2H"},
+        "gpu_launches": int(np.mean([s_["kernel_launches"] for s_ in stats])),
+        "plain_fp64": {"solves_per_s": round(plain_sps, 6), "ms_per_solve": round(plain_ms, 1),
+                       "sample": f"{ncol} of {R} columns, per-RHS cold start, extrapolated",
+                       "iters_max": int(stp["iters_max"])},
+        "speedup_vs_plain_fp64": round(value / plain_sps, 2),
+        "solve": {"iters_max": [int(s_["iters_max"]) for s_ in stats],
+                  "iters_max_cold_first_step": int(cold["iters_max"]) if cold else None,
+                  "refinements": [int(s_["refinements"]) for s_ in stats],
+                  "true_relres_max": max(s_["true_relres_max"] for s_ in stats),
+                  "n_converged": [int(s_["n_converged"]) for s_ in stats]},
+        "host_plan_ms": round(t_plan * 1000, 1),
+        "roofline": roofline,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(scenes[args.warmup], st)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _matvec_roofline(st, nf, n, R, matvec):
+    """Roofline of the dominant kernel (the K / K^T matvec) from live CUDA
+    events of the timed solve: algorithmic flops nf*n*(20 + 2R) per launch."""
+    hbm, bf16, src = _peaks()
+    launch_ms = st["t_matvec_ms"] / max(1, st["n_matvec"])
+    flops = float(nf) * n * (20 + 2 * R)
+    achieved = flops / (launch_ms * 1e-3) / 1e12
+    return {"bound": "tensor", "achieved": round(achieved, 2), "peak": bf16, "unit": "TFLOP/s",
+            "frac": round(achieved / bf16, 4), "traffic": None,
+            "kernel": ("pk_tc_kernel<0|1> (tcgen05 3xTF32, TMEM accumulators)" if matvec != "simt"
+                       else "pk_rows_kernel / pk_cols_kernel (FP32 SIMT)"),
+            "launch_ms": round(launch_ms, 3), "peak_source": f"bf16 dense, {src} (of measured)"}
 
 
 def run_ours(args):
@@ -322,14 +508,24 @@ def run_probe(args):
 
     import fastmbcui_b200 as F
 
-    build, desc = WORKLOADS[args.workload]
-    sc = build(4)
+    sc = _scene_for(args.workload, 4)
     R = 6 * sc.n_bodies
     dev = torch.device("cuda", 0)
     t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
     plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
     solver = F.Solver(plan, x=t(sc.x), nx=t(sc.nx), y=t(sc.y), coef=sc.coef, precision=F.MBC_F32)
     solver.set_matvec(MATVEC[args.matvec]).factor()
+    if args.probe_solve:
+        # one complete mixed solve (the launch list of a step)
+        Fm = t(sc.rhs())
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        X, st = solver.solve(Fm, out_dtype=torch.float32, tol=1e-8, max_iters=args.max_iters, max_refine=64,
+                             inner_tol=1e-2, check_every=8, profile=1)
+        torch.cuda.synchronize()
+        st["wall_ms"] = (time.perf_counter() - t0) * 1000
+        print(json.dumps({"probe_solve": args.workload, "R": R, "stats": st}), flush=True)
+        return
     rng = np.random.default_rng(0)
     V = t(rng.standard_normal((sc.n, R)))
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
@@ -354,8 +550,8 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    build, desc = WORKLOADS[args.workload]
-    sc = build(4)
+    desc = WORKLOADS[args.workload][1]
+    sc = _scene_for(args.workload, 4)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
@@ -388,15 +584,20 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ellipsoids32", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="trajectory32", choices=sorted(WORKLOADS))
     ap.add_argument("--max-iters", type=int, default=3000)
     ap.add_argument("--plain-cols", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--ref-iters", type=int, default=200)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--warm", default="previous", choices=["learned", "previous", "cold"],
+                    help="trajectory warm start")
+    ap.add_argument("--warm-model", default=os.path.join(ROOT, "fastmbcui_b200", "data", "warmstart_mlp.npz"))
     ap.add_argument("--kernel-probe", action="store_true",
                     help="only run a factor and a few K / K^T launches (ncu captures)")
     ap.add_argument("--probe-reps", type=int, default=3)
+    ap.add_argument("--probe-solve", action="store_true",
+                    help="with --kernel-probe: one full mixed solve instead of K / K^T launches")
     ap.add_argument("--matvec", default="auto", choices=sorted(MATVEC),
                     help="FP32 matvec: tensor cores (3xTF32 tcgen05) or CUDA cores")
     args = ap.parse_args()
@@ -404,6 +605,8 @@ def main():
         run_probe(args)
     elif args.impl == "reference":
         run_reference(args)
+    elif args.workload == "trajectory32":
+        run_trajectory(args)
     else:
         run_ours(args)
 
