@@ -240,3 +240,31 @@ class Solver:
                                     None if frc is None else frc.ctypes.data, self._sp()),
               "mbc_added_mass")
         return (Mf, frc) if accel is not None else Mf
+
+
+def solve_many(solvers, Fs, X0s=None, threads=None, factor=True, **opts):
+    """Factor and solve independent scenes concurrently: each solver on its
+    own CUDA stream, driven by its own host thread (the library's calls
+    release the interpreter lock), so small scenes fill the GPU together.
+    Returns [(X, stats)] in input order.  Results are bitwise those of
+    solving the scenes one by one: every kernel reduces in a fixed order."""
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+
+    dev = torch.cuda.current_device()
+    X0s = list(X0s) if X0s is not None else [None] * len(solvers)
+    producer = torch.cuda.current_stream()
+
+    def work(i):
+        torch.cuda.set_device(dev)
+        st = torch.cuda.Stream()
+        st.wait_stream(producer)  # the inputs were made on the caller's stream
+        with torch.cuda.stream(st):
+            if factor:
+                solvers[i].factor()
+            X, stats = solvers[i].solve(Fs[i], X0=X0s[i], **opts)
+        st.synchronize()
+        return X, stats
+
+    with ThreadPoolExecutor(max_workers=threads or min(8, max(1, len(solvers)))) as ex:
+        return list(ex.map(work, range(len(solvers))))

@@ -43,7 +43,8 @@ class Operator(C.Structure):
 class SolveOptions(C.Structure):
     _fields_ = [("max_iters", C.c_int32), ("tol", C.c_double), ("schedule", C.c_int32),
                 ("precondition", C.c_int32), ("max_refine", C.c_int32), ("inner_tol", C.c_double),
-                ("check_every", C.c_int32), ("true_residual", C.c_int32), ("profile", C.c_int32)]
+                ("check_every", C.c_int32), ("true_residual", C.c_int32), ("profile", C.c_int32),
+                ("graph", C.c_int32)]
 
 
 class SolveStats(C.Structure):
@@ -52,7 +53,7 @@ class SolveStats(C.Structure):
                 ("n_converged", C.c_int32), ("relres_max", C.c_double),
                 ("true_relres_max", C.c_double), ("t_solve_ms", C.c_double),
                 ("t_matvec_ms", C.c_double), ("n_matvec", C.c_int64), ("kernel_launches", C.c_int64),
-                ("n_polished", C.c_int32)]
+                ("n_polished", C.c_int32), ("t_matvec64_ms", C.c_double), ("n_matvec64", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -44,6 +44,23 @@ namespace mbc {
 
 static inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
+// Opt a kernel in to the device's largest dynamic shared memory.  The limit
+// is per-kernel state shared by every host thread; setting it to one fixed
+// value (rather than to each launch's own size) keeps concurrent solvers
+// from lowering it under one another's launches.
+template <typename K>
+static mbc_status allow_max_smem(K kern, size_t need)
+{
+  int dev = 0, cap = 0;
+  MBC_CK(cudaGetDevice(&dev));
+  MBC_CK(cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (need > (size_t)cap)
+    return fail(MBC_UNSUPPORTED, "kernel needs " + std::to_string(need) + " B of shared memory, device allows " +
+                                     std::to_string(cap));
+  MBC_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
+  return MBC_OK;
+}
+
 DevMem::~DevMem() { release(); }
 void DevMem::release()
 {
@@ -154,6 +171,10 @@ static bool use_tc(const Solver &S, int R)
   const int np = (R + 15) / 16 * 16;
   const int K = std::max(S.n, S.nf);
   const size_t need = (size_t)cdiv(K, tc::kK) * 2 * tc::tile_b_bytes(np);
+  // both directions must fit the device's shared memory (true on sm_100a)
+  if (allow_max_smem(tc::pk_tc_kernel<0>, tc::smem_bytes(np, 0)) != MBC_OK ||
+      allow_max_smem(tc::pk_tc_kernel<1>, tc::smem_bytes(np, 1)) != MBC_OK)
+    return false;
   return S.m_bimg.reserve(need) == MBC_OK;
 }
 
@@ -183,8 +204,7 @@ static int tc_launch(const Solver &S, int R, const float *vin, float *out, const
   const int64_t pack_threads = (int64_t)nks * a.np * (tc::kK / 4);
   tc::pack_b_kernel<<<cdiv(pack_threads, 256), 256, 0, st>>>(vin, K, R, a.np, nks, (uint4 *)S.m_bimg.ptr,
                                                               done);
-  const int smem = tc::smem_bytes(a.np, DIR);
-  cudaFuncSetAttribute(tc::pk_tc_kernel<DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const int smem = tc::smem_bytes(a.np, DIR);  // allowed by use_tc
   const unsigned grid = cdiv(M, tc::kM);
   tc::pk_tc_kernel<DIR><<<grid, tc::kThreads, smem, st>>>(a);
   return (int)grid;
@@ -268,7 +288,7 @@ template <typename T, typename LT, int NT, int EPT>
 mbc_status launch_factor_class(FactorArgs a, T *theta, LT *lval, size_t smem, cudaStream_t st)
 {
   auto kern = factor_kernel<T, LT, NT, EPT>;
-  MBC_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  MBC_TRY(allow_max_smem(kern, smem));
   kern<<<a.count, NT, smem, st>>>(a, theta, lval);
   MBC_CKL();
   return MBC_OK;
@@ -570,6 +590,19 @@ static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, XT *x, const LT *lval
                           cudaStream_t st, const double *d_b2ref,
                           const std::function<mbc_status()> *replace, int max_replace)
 {
+  // Blocks of check_every iterations have fixed kernel arguments (scalars
+  // live on the device), so with S.graph a full block is captured once as a
+  // CUDA graph and replayed: one launch per block instead of ~9 per
+  // iteration, which matters for small scenes.  The first block runs
+  // eagerly (it sizes every buffer); profiling runs eagerly throughout.
+  struct GraphGuard {
+    cudaGraphExec_t exec = nullptr;
+    ~GraphGuard()
+    {
+      if (exec) cudaGraphExecDestroy(exec);
+    }
+  } graph;
+  int64_t graph_launches = 0;
   const Layout2D L = layout2d(S.n, R);
   const int nblk2 = (int)L.grid.x;
   w.sc.maxit = maxit;
@@ -588,7 +621,14 @@ static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, XT *x, const LT *lval
   int replaced = 0;
   for (int it = 0; it < maxit; it += check_every) {
     const int kmax = std::min(check_every, maxit - it);
-    for (int k = 0; k < kmax; ++k) {
+    const bool use_graph = S.graph && !S.profile && it > 0 && kmax == check_every;
+    if (use_graph && graph.exec) {
+      MBC_CK(cudaGraphLaunch(graph.exec, st));
+      S.launches += graph_launches;
+    }
+    const int64_t launches_before = S.launches;
+    if (use_graph && !graph.exec) MBC_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+    for (int k = 0; k < kmax && !(use_graph && graph.exec && graph_launches > 0); ++k) {
       if (precond) {
         precond_lt_kernel<T, LT><<<L.grid, L.block, 0, st>>>(S.n, R, S.d_lptr(), S.d_lind(), lval,
                                                               w.Rv, w.U, w.sc.done);
@@ -612,6 +652,16 @@ static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, XT *x, const LT *lval
       reduce_kernel<<<1, 1024, 0, st>>>(nblk2, R, w.part, RED_CHECK, w.sc, nullptr);
       S.launches += precond ? 9 : 8;
     }
+    if (use_graph && !graph.exec) {
+      cudaGraph_t g = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(st, &g);
+      if (ec != cudaSuccess) return fail(MBC_CUDA_ERROR, std::string("capture of a PCG block: ") + cudaGetErrorString(ec));
+      const cudaError_t ei = cudaGraphInstantiate(&graph.exec, g, 0);
+      cudaGraphDestroy(g);
+      if (ei != cudaSuccess) return fail(MBC_CUDA_ERROR, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ei));
+      graph_launches = S.launches - launches_before;
+      MBC_CK(cudaGraphLaunch(graph.exec, st));
+    }
     MBC_CKL();
     MBC_CK(cudaMemcpyAsync(h_flags, w.sc.done, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     MBC_CK(cudaStreamSynchronize(st));
@@ -622,6 +672,7 @@ static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, XT *x, const LT *lval
         float ms = 0.f;
         MBC_CK(cudaEventElapsedTime(&ms, S.events[2 * k], S.events[2 * k + 1]));
         S.prof_ms_all.push_back(ms);
+        S.prof_is64.push_back(sizeof(T) == 8 ? 1 : 0);
       }
     }
     if (h_flags[0]) break;
@@ -999,7 +1050,9 @@ mbc_status Solver::solve(int R, const void *rhs, int32_t rhs_dt, void *X, int32_
   const auto t0 = std::chrono::steady_clock::now();
   const int64_t launches0 = launches;
   profile = o.profile != 0;
+  graph = o.graph != 0;
   prof_ms_all.clear();
+  prof_is64.clear();
   mbc_status rs;
   if (o.schedule == MBC_SCHED_PER_RHS && R > 1) {
     // one cold-started PCG per column, in order (mfs_torch_ops.cu:166-171)
@@ -1056,16 +1109,25 @@ mbc_status Solver::solve(int R, const void *rhs, int32_t rhs_dt, void *X, int32_
     stats->kernel_launches = launches - launches0;
     stats->t_matvec_ms = 0;
     stats->n_matvec = 0;
+    stats->t_matvec64_ms = 0;
+    stats->n_matvec64 = 0;
     if (profile) {
       // a matvec pair whose kernels exited on the done flag takes a few
-      // microseconds; count only pairs that did work (> 1% of the longest)
-      float mx = 0.f;
-      for (float v : prof_ms_all) mx = std::max(mx, v);
-      for (float v : prof_ms_all)
-        if (v > 0.01f * mx) {
-          stats->t_matvec_ms += v;
+      // microseconds; count only pairs that did work (> 1% of the longest of
+      // the same precision)
+      float mx[2] = {0.f, 0.f};
+      for (size_t i = 0; i < prof_ms_all.size(); ++i) mx[prof_is64[i]] = std::max(mx[prof_is64[i]], prof_ms_all[i]);
+      for (size_t i = 0; i < prof_ms_all.size(); ++i) {
+        const int p64 = prof_is64[i];
+        if (prof_ms_all[i] > 0.01f * mx[p64]) {
+          stats->t_matvec_ms += prof_ms_all[i];
           stats->n_matvec += 2;
+          if (p64) {
+            stats->t_matvec64_ms += prof_ms_all[i];
+            stats->n_matvec64 += 2;
+          }
         }
+      }
     }
   }
   MBC_TRY(check_device_error(st));
@@ -1206,6 +1268,8 @@ extern "C" void mbc_solve_default_options(mbc_solve_options *o)
   o->inner_tol = 1e-2;
   o->check_every = 8;
   o->true_residual = 0;
+  o->profile = 0;
+  o->graph = 0;
 }
 
 static mbc_status check_solve_args(mbc_solver *s, int32_t R, const void *in, int32_t in_dt, void *X,

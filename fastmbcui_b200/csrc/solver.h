@@ -32,9 +32,11 @@ struct Solver {
   int64_t launches = 0;       // kernels launched by this solver (solve paths)
   int32_t replacements = 0;   // residual replacements in the last PCG run
   bool profile = false;
+  bool graph = false;  // replay PCG iteration blocks as CUDA graphs
   int32_t matvec_impl = MBC_MATVEC_AUTO;
   std::vector<cudaEvent_t> events;
   std::vector<float> prof_ms_all;
+  std::vector<int> prof_is64;  // 1: the pair ran in FP64
 
   // plan on the device
   DevMem m_P, m_Pinv, m_sup_ptr, m_sup_ind, m_set_ptr, m_set_ind, m_lptr, m_lind, m_rptr, m_rcol,

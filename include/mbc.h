@@ -158,6 +158,8 @@ typedef struct {
   int32_t check_every;   /* iterations between convergence checks on the host */
   int32_t true_residual; /* 1 = report the FP64-recomputed |K^T(f-Kx)|/|K^T f| */
   int32_t profile;       /* 1 = time the matvec kernels with CUDA events on `stream` */
+  int32_t graph;         /* 1 = replay blocks of check_every PCG iterations as a CUDA graph
+                            (captured on the first full block; ignored with profile) */
 } mbc_solve_options;
 
 typedef struct {
@@ -174,6 +176,8 @@ typedef struct {
   int64_t kernel_launches;  /* kernels this call launched */
   int32_t n_polished;       /* MBC_F32: columns finished by FP64 PCG after the FP32
                                recursion stagnated or ran out of iterations */
+  double t_matvec64_ms;     /* profile: the FP64 part of t_matvec_ms */
+  int64_t n_matvec64;       /* profile: FP64 K / K^T launches timed */
 } mbc_solve_stats;
 
 void mbc_solve_default_options(mbc_solve_options *opt);
