@@ -54,10 +54,13 @@ static mbc_status allow_max_smem(K kern, size_t need)
   int dev = 0, cap = 0;
   MBC_CK(cudaGetDevice(&dev));
   MBC_CK(cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  if (need > (size_t)cap)
-    return fail(MBC_UNSUPPORTED, "kernel needs " + std::to_string(need) + " B of shared memory, device allows " +
-                                     std::to_string(cap));
-  MBC_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
+  cudaFuncAttributes fa;
+  MBC_CK(cudaFuncGetAttributes(&fa, kern));
+  const int dyn_cap = cap - (int)fa.sharedSizeBytes;  // static + dynamic <= the opt-in cap
+  if (need > (size_t)std::max(dyn_cap, 0))
+    return fail(MBC_UNSUPPORTED, "kernel needs " + std::to_string(need) + " B of dynamic shared memory, device allows " +
+                                     std::to_string(dyn_cap));
+  MBC_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_cap));
   return MBC_OK;
 }
 
@@ -621,7 +624,9 @@ static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, XT *x, const LT *lval
   int replaced = 0;
   for (int it = 0; it < maxit; it += check_every) {
     const int kmax = std::min(check_every, maxit - it);
-    const bool use_graph = S.graph && !S.profile && it > 0 && kmax == check_every;
+    // (the captured block holds kernel launches only: the unpreconditioned
+    // variant's checked copy and the profiling events stay eager)
+    const bool use_graph = S.graph && precond && !S.profile && it > 0 && kmax == check_every;
     if (use_graph && graph.exec) {
       MBC_CK(cudaGraphLaunch(graph.exec, st));
       S.launches += graph_launches;

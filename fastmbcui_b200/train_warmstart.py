@@ -47,10 +47,38 @@ def generate(pts, steps, seed, tol=1e-8, n_bodies=32):
     return np.stack(feats), np.stack(targs), iters
 
 
-def train(feats, targs, epochs=400, batch=1024, lr=1e-3, seed=0, hold=0.25):
+def generate_cold(pts, steps, seed, tol=1e-8, n_bodies=32, stride=1):
+    """Cold-start samples: for the poses of a trajectory, the pair features of
+    each pose and the blocks H with U H = the solved strengths."""
+    import torch
+
+    from . import Plan, Solver, _lib
+    from . import scenes as S
+    from . import warmstart as W
+
+    base, q, _ = S.trajectory_scene(n_bodies, pts, seed=seed, steps=steps * stride + 1)
+    U = W.isolated_basis(base)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device="cuda")
+    X_prev, feats, targs = None, [], []
+    for k in range(0, steps * stride, stride):
+        sc = S.moved(base, q[k])
+        plan = Plan(sc.y, sc.rho, sc.lam, sc.max_super)
+        s = Solver(plan, x=t(sc.x), nx=t(sc.nx), y=t(sc.y), coef=sc.coef, precision=_lib.MBC_F32).factor()
+        X, _ = s.solve(t(sc.rhs()), X0=X_prev, out_dtype=torch.float32, tol=tol, max_iters=4000,
+                       max_refine=64, inner_tol=1e-2)
+        pairs = W.neighbour_pairs(sc.centers)
+        feats.append(W.cold_features(pairs, q[k], base.centers, base.meta["axes"], base.meta["rot"]))
+        targs.append(W.pair_targets(U, X, base, pairs).cpu().numpy())
+        X_prev = X
+    return np.stack(feats), np.stack(targs)
+
+
+def train(feats, targs, epochs=400, batch=1024, lr=1e-3, seed=0, hold=0.25, cls=None):
     import torch
 
     from .warmstart import Mlp, WarmStart
+
+    cls = cls or WarmStart
 
     T = feats.shape[0]
     n_tr = max(1, int(round(T * (1 - hold))))
@@ -71,7 +99,7 @@ def train(feats, targs, epochs=400, batch=1024, lr=1e-3, seed=0, hold=0.25):
             loss = net.train_step(xs[idx], ys[idx], lr=lr)
         if ep % 50 == 0 or ep == epochs - 1:
             hist.append((ep, loss))
-    ws = WarmStart(net, x_mean, x_std, y_std)
+    ws = cls(net, x_mean, x_std, y_std)
 
     def rel_err(X, Y):
         if X.shape[0] == 0:

@@ -187,3 +187,70 @@ class WarmStart:
         net = Mlp(dims[0], dims[-1], hidden=dims[1], layers=len(dims) - 2)
         net.set_params(z["params"])
         return cls(net, z["x_mean"], z["x_std"], float(z["y_std"]))
+
+
+# --------------------------------------------------------------------------
+# Learned cold start: a scene with no history (the first step of a
+# trajectory, an independent scene of a batch).  x0 = U H over the pairs
+# (c, b): for c = b the block that turns the isolated solution of body b into
+# its share of the coupled one, for its neighbours c the response of body c to
+# the motion of body b, both predicted from the pair's geometry.
+# --------------------------------------------------------------------------
+
+N_COLD_FEATURES = 36
+
+
+def cold_features(pairs, q_cur, base_centers, axes, base_rot):
+    """Network inputs (P x N_COLD_FEATURES) of the pairs (c, b) of one pose."""
+    from .scenes import rotvec_matrix
+
+    q_cur = np.asarray(q_cur, np.float64)
+    cen = np.asarray(base_centers, np.float64) + q_cur[:, :3]
+    Rq = [rotvec_matrix(q_cur[b, 3:6]) for b in range(q_cur.shape[0])]
+    Rw = [Rq[b] @ base_rot[b] for b in range(q_cur.shape[0])]
+    f = np.zeros((len(pairs), N_COLD_FEATURES))
+    for i, (c, b) in enumerate(pairs):
+        d = cen[c] - cen[b]
+        r = float(np.linalg.norm(d))
+        inv = 1.0 / r if r > 0 else 0.0
+        f[i] = np.concatenate([d * inv, [inv, inv ** 3, 1.0 if c == b else 0.0], Rw[b].ravel(), Rw[c].ravel(),
+                               axes[b], axes[c], q_cur[b, 3:6], q_cur[c, 3:6]])
+    return f.astype(np.float32)
+
+
+class ColdStart(WarmStart):
+    """x0 = U H for a scene without history (H from the network)."""
+
+    def start(self, n, R, U, src_body_dev, n_bodies, pairs, feats):
+        import torch
+
+        X0 = torch.zeros((n, R), dtype=torch.float32, device=U.device)
+        Hp = self.predict_H(feats)
+        H = torch.zeros((n_bodies * n_bodies, 36), dtype=torch.float32, device=U.device)
+        idx = torch.as_tensor(pairs[:, 0].astype(np.int64) * n_bodies + pairs[:, 1], device=U.device)
+        H[idx] = Hp
+        check(load().mbc_warm_correct(n, R, src_body_dev.data_ptr(), n_bodies, U.data_ptr(), H.data_ptr(),
+                                      X0.data_ptr(), C.c_void_p(torch.cuda.current_stream().cuda_stream)),
+              "mbc_warm_correct")
+        return X0
+
+
+def isolated_start(n, R, U, src_body_dev, n_bodies, q_cur):
+    """x0 = each body's own isolated solution, rotated to its pose (no network)."""
+    import torch
+
+    from .scenes import rotvec_matrix
+
+    H = np.zeros((n_bodies * n_bodies, 36), np.float32)
+    for b in range(n_bodies):
+        RqT = rotvec_matrix(np.asarray(q_cur[b, 3:6], np.float64)).T
+        G = np.zeros((6, 6))
+        G[:3, :3] = RqT
+        G[3:, 3:] = RqT
+        H[b * n_bodies + b] = G.ravel()
+    X0 = torch.zeros((n, R), dtype=torch.float32, device=U.device)
+    Hd = torch.as_tensor(H, device=U.device)
+    check(load().mbc_warm_correct(n, R, src_body_dev.data_ptr(), n_bodies, U.data_ptr(), Hd.data_ptr(),
+                                  X0.data_ptr(), C.c_void_p(torch.cuda.current_stream().cuda_stream)),
+          "mbc_warm_correct")
+    return X0
