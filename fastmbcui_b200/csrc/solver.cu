@@ -975,7 +975,7 @@ mbc_status Solver::solve_mixed(int R, const void *rhs, int32_t rhs_dt, void *X, 
                                          o.precondition != 0, std::max(1, o.check_every), nullptr, st,
                                          (const double *)b2ref.ptr, &replace, max_replace)));
   // final true residual for every column (the status of columns that hit
-  // max_iters is re-judged on it)
+  // max_iters is decided on it)
   MBC_TRY(replace());
   std::vector<int32_t> status, iters;
   std::vector<double> rel;
@@ -1015,7 +1015,7 @@ mbc_status Solver::solve_mixed(int R, const void *rhs, int32_t rhs_dt, void *X, 
     MBC_CKL();
     MBC_CK(cudaStreamSynchronize(st));
     for (int k = 0; k < Rs; ++k) iters[pol[k]] += it64[k];
-    // judge every polished column on its FP64 true residual
+    // every polished column is decided on its FP64 true residual
     MBC_TRY(true_residual_into_r());
     std::vector<double> nr, nb;
     MBC_TRY(col_norms2<double>(*this, R, Rd, nr, st));

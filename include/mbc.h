@@ -225,7 +225,7 @@ mbc_status mbc_added_mass(mbc_solver *s, int32_t R, const void *X, int32_t x_dty
 /* Warm-start network: a small MLP trained and evaluated on the GPU by this  */
 /* library's own kernels.  No counterpart in the reference (its PCG always   */
 /* starts from x0 = 0, kl_chol.cu:930-940): the network predicts a warm      */
-/* start that the PCG then refines, with the FP64 true residual as judge.     */
+/* start that the PCG then refines to the same FP64 true-residual criterion. */
 /* Layers n_in -> hidden (tanh) x n_hidden_layers -> n_out (linear); BF16     */
 /* weights in the products, FP32 accumulation, FP32 master weights + Adam.   */
 /* Parameter vector layout: per layer W (row-major out x in), then b.        */
