@@ -599,7 +599,9 @@ def run_probe(args):
     dev = torch.device("cuda", 0)
     t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
     plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
-    solver = F.Solver(plan, x=t(sc.x), nx=t(sc.nx), y=t(sc.y), coef=sc.coef, precision=F.MBC_F32)
+    f64 = args.probe_precision == "f64"
+    solver = F.Solver(plan, x=t(sc.x), nx=t(sc.nx), y=t(sc.y), coef=sc.coef,
+                      precision=F.MBC_F64 if f64 else F.MBC_F32)
     solver.set_matvec(MATVEC[args.matvec]).factor()
     if args.probe_solve:
         # one complete mixed solve (the launch list of a step)
@@ -614,6 +616,8 @@ def run_probe(args):
         return
     rng = np.random.default_rng(0)
     V = t(rng.standard_normal((sc.n, R)))
+    if f64:
+        V = V.double()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     out = []
     for _ in range(args.probe_reps):
@@ -624,7 +628,8 @@ def run_probe(args):
         ev[2].record()
         torch.cuda.synchronize()
         out.append((ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])))
-    print(json.dumps({"probe": args.workload, "matvec": args.matvec, "R": R,
+    print(json.dumps({"probe": args.workload, "matvec": "simt" if f64 else args.matvec,
+                      "precision": args.probe_precision, "R": R,
                       "K_ms": [round(a, 3) for a, _ in out],
                       "KT_ms": [round(b, 3) for _, b in out]}), flush=True)
 
@@ -685,6 +690,8 @@ def main():
     ap.add_argument("--kernel-probe", action="store_true",
                     help="only run a factor and a few K / K^T launches (ncu captures)")
     ap.add_argument("--probe-reps", type=int, default=3)
+    ap.add_argument("--probe-precision", default="f32", choices=["f32", "f64"],
+                    help="with --kernel-probe: the FP32 matvec (tensor or SIMT) or the FP64 SIMT matvec")
     ap.add_argument("--probe-solve", action="store_true",
                     help="with --kernel-probe: one full mixed solve instead of K / K^T launches")
     ap.add_argument("--matvec", default="auto", choices=sorted(MATVEC),
