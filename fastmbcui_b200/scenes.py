@@ -102,6 +102,13 @@ class Scene:
 
 def icosphere(subdiv: int) -> np.ndarray:
     """Unit icosphere vertices (10*4^subdiv + 2), deterministic order."""
+    return icosphere_mesh(subdiv)[0]
+
+
+def icosphere_mesh(subdiv: int):
+    """Unit icosphere: vertices (10*4^subdiv + 2, deterministic order) and
+    triangles (20*4^subdiv x 3, int32) ordered counter-clockwise seen from
+    outside, so that (v1 - v0) x (v2 - v0) points outward."""
     t = (1.0 + 5.0 ** 0.5) / 2.0
     v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t),
          (0, -1, -t), (0, 1, -t), (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
@@ -125,7 +132,7 @@ def icosphere(subdiv: int) -> np.ndarray:
             ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
             nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
         faces = nf
-    return np.array(verts)
+    return np.array(verts), np.array(faces, dtype=np.int32)
 
 
 def sample_cylinder(rng: np.random.Generator, npts: int, r: float, h: float):

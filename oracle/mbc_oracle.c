@@ -678,6 +678,75 @@ void orc_added_mass(int nf, int n, const double *x, const double *nx, const doub
   free(phi);
 }
 
+/*
+ * Mesh collocation operator: the solid angle of face f seen from source j
+ * (utils/torch_utils.py:306-334, compute_solid_angle; van Oosterom and
+ * Strackee), Rk = V[F[f, k]] - S[j]:
+ *   M[f, j] = 2 atan2(R1 . (R2 x R3), l1 l2 l3 + (R1.R2) l3 + (R1.R3) l2 + (R2.R3) l1).
+ * Rows: every face (bodies concatenated, core/KTAB_Mfs_spclf1d.py:112);
+ * columns: every source.  M is row-major n_faces x n_src.
+ */
+void orc_mesh_solid_angle(int n_faces, const double *V, const int32_t *F, int n_src, const double *S,
+                          double *M)
+{
+  int f;
+#pragma omp parallel for schedule(static)
+  for (f = 0; f < n_faces; ++f) {
+    const double *v1 = &V[3 * F[3 * f]], *v2 = &V[3 * F[3 * f + 1]], *v3 = &V[3 * F[3 * f + 2]];
+    int j;
+    for (j = 0; j < n_src; ++j) {
+      const double *s = &S[3 * j];
+      const double a[3] = {v1[0] - s[0], v1[1] - s[1], v1[2] - s[2]};
+      const double b[3] = {v2[0] - s[0], v2[1] - s[1], v2[2] - s[2]};
+      const double c[3] = {v3[0] - s[0], v3[1] - s[1], v3[2] - s[2]};
+      const double bxc[3] = {b[1] * c[2] - b[2] * c[1], b[2] * c[0] - b[0] * c[2], b[0] * c[1] - b[1] * c[0]};
+      const double num = a[0] * bxc[0] + a[1] * bxc[1] + a[2] * bxc[2];
+      const double la = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+      const double lb = sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+      const double lc = sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+      const double ab = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+      const double ac = a[0] * c[0] + a[1] * c[1] + a[2] * c[2];
+      const double bc = b[0] * c[0] + b[1] * c[1] + b[2] * c[2];
+      const double den = la * lb * lc + ab * lc + ac * lb + bc * la;
+      M[(size_t)f * n_src + j] = 2.0 * atan2(num, den);
+    }
+  }
+}
+
+/*
+ * Rigid-mode right-hand side of the mesh operator: FL @ IQ of
+ * core/KTAB_Mfs_spclf1d.py:101-108 with compute_FL_matrix
+ * (utils/torch_utils.py:62-75) and compute_face_centers (:49-60).  Face f of
+ * body b has the area-weighted normal s = (v2 - v1) x (v3 - v1) / 2 and the
+ * lever arm r = (v1 + v2 + v3) / 3 - y_b; FL's row (r x s, s) times
+ * IQ = [[0, I], [I, 0]] puts (s, r x s) in columns 6b .. 6b + 5.
+ * Out: row-major n_faces x 6 n_bodies, zero outside the face's body block.
+ */
+void orc_mesh_rhs(int n_faces, const double *V, const int32_t *F, const int32_t *face_body, int n_bodies,
+                  const double *body_pos, double *out)
+{
+  int f;
+  memset(out, 0, sizeof(double) * (size_t)n_faces * 6 * n_bodies);
+  for (f = 0; f < n_faces; ++f) {
+    const double *v1 = &V[3 * F[3 * f]], *v2 = &V[3 * F[3 * f + 1]], *v3 = &V[3 * F[3 * f + 2]];
+    const int b = face_body[f];
+    const double e1[3] = {v2[0] - v1[0], v2[1] - v1[1], v2[2] - v1[2]};
+    const double e2[3] = {v3[0] - v1[0], v3[1] - v1[1], v3[2] - v1[2]};
+    const double sv[3] = {(e1[1] * e2[2] - e1[2] * e2[1]) / 2.0, (e1[2] * e2[0] - e1[0] * e2[2]) / 2.0,
+                          (e1[0] * e2[1] - e1[1] * e2[0]) / 2.0};
+    const double r[3] = {(v1[0] + v2[0] + v3[0]) / 3.0 - body_pos[3 * b],
+                         (v1[1] + v2[1] + v3[1]) / 3.0 - body_pos[3 * b + 1],
+                         (v1[2] + v2[2] + v3[2]) / 3.0 - body_pos[3 * b + 2]};
+    double *o = out + (size_t)f * 6 * n_bodies + 6 * b;
+    o[0] = sv[0];
+    o[1] = sv[1];
+    o[2] = sv[2];
+    o[3] = r[1] * sv[2] - r[2] * sv[1];
+    o[4] = r[2] * sv[0] - r[0] * sv[2];
+    o[5] = r[0] * sv[1] - r[1] * sv[0];
+  }
+}
+
 int orc_num_threads(void)
 {
 #ifdef _OPENMP

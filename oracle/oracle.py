@@ -56,6 +56,10 @@ def lib():
         L.orc_factor.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, C.c_double, _i32p, C.c_int,
                                  _i32p, _i32p, _i32p, _i32p, _i64p, _f64p, _i32p, _i32p, _f64p,
                                  C.POINTER(C.c_int32)]
+        L.orc_mesh_solid_angle.argtypes = [C.c_int, _f64p, _i32p, C.c_int, _f64p, _f64p]
+        L.orc_mesh_solid_angle.restype = None
+        L.orc_mesh_rhs.argtypes = [C.c_int, _f64p, _i32p, _i32p, C.c_int, _f64p, _f64p]
+        L.orc_mesh_rhs.restype = None
         L.orc_added_mass.argtypes = [C.c_int, C.c_int, _f64p, _f64p, _f64p, C.c_int, _f64p, _f64p, C.c_int,
                                      _i32p, _f64p, C.c_double, _f64p]
         L.orc_added_mass.restype = None
@@ -287,6 +291,20 @@ def added_mass(sc, X, rho_f=1.0):
     lib().orc_added_mass(sc.nf, sc.n, f(sc.x), f(sc.nx), f(sc.y), R, X, f(sc.weights()), nb,
                          np.ascontiguousarray(sc.body_ptr(), np.int32), f(sc.centers), float(rho_f), out)
     return out
+
+
+def mesh_operator(V, F, face_body, body_pos, S):
+    """Solid-angle matrix (faces x sources) and rigid-mode right-hand side
+    FL @ IQ (faces x 6 bodies) of a triangle-mesh scene, FP64."""
+    f = lambda a: np.ascontiguousarray(a, np.float64)
+    i = lambda a: np.ascontiguousarray(a, np.int32)
+    V, F, S, fb, bp = f(V), i(F), f(S), i(face_body), f(body_pos)
+    nfc, ns, nb = F.shape[0], S.shape[0], bp.shape[0]
+    M = np.empty((nfc, ns))
+    rhs = np.empty((nfc, 6 * nb))
+    lib().orc_mesh_solid_angle(nfc, V, F, ns, S, M)
+    lib().orc_mesh_rhs(nfc, V, F, fb, nb, bp, rhs)
+    return M, rhs
 
 
 def num_threads() -> int:
