@@ -95,6 +95,8 @@ SIGNATURES = {
     "mbc_mlp_forward": (C.c_int, [_vp, _i32, _vp, _vp, _vp]),
     "mbc_mlp_train_step": (C.c_int, [_vp, _i32, _vp, _vp, C.c_float, _vp, _vp, _vp]),
     "mbc_warm_correct": (C.c_int, [_i32, _i32, _vp, _i32, _vp, _vp, _vp, _vp]),
+    "mbc_mesh_assemble": (C.c_int, [_i32, _vp, _i32, _vp, _vp, _i32, _vp, _i32, _vp, _i32, _vp, _i64, _vp,
+                                    _vp]),
     "mbc_point_apply_noalloc": (C.c_int, [_i32, _i32, _i32, _vp, _vp, _vp, C.c_double, _i32, _vp, _vp, _vp]),
     "mbc_context_create": (C.c_int, [C.POINTER(_vp)]),
     "mbc_context_destroy": (C.c_int, [_vp]),

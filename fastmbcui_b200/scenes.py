@@ -422,3 +422,45 @@ def trajectory_scene(n_bodies: int = 32, pts: int = 2000, seed: int = 4, steps: 
                            "rot": np.array(rots)})
     q, v = trajectory_poses(n_bodies, steps, seed + 1, dt, amp_range)
     return base, q, v
+
+
+def vertex_normals(V, F) -> np.ndarray:
+    """Unit vertex normals of a triangle mesh: face normals summed with the
+    angle of each face at the vertex as weight."""
+    V = np.asarray(V, np.float64)
+    p0, p1, p2 = V[F[:, 0]], V[F[:, 1]], V[F[:, 2]]
+    fn = np.cross(p1 - p0, p2 - p0)
+    fn /= np.linalg.norm(fn, axis=1, keepdims=True)
+
+    def angle(a, b):
+        c = np.einsum("ij,ij->i", a, b) / (np.linalg.norm(a, axis=1) * np.linalg.norm(b, axis=1))
+        return np.arccos(np.clip(c, -1.0, 1.0))
+
+    ang = [angle(p1 - p0, p2 - p0), angle(p0 - p1, p2 - p1), angle(p0 - p2, p1 - p2)]
+    acc = np.zeros_like(V)
+    for k in range(3):
+        np.add.at(acc, F[:, k], fn * ang[k][:, None])
+    return acc / np.linalg.norm(acc, axis=1, keepdims=True)
+
+
+def mesh_scene(bodies):
+    """Triangle-mesh bodies, each (subdivision, semi-axes, rotation vector,
+    position, source offset): a scaled, turned icosphere with one source per
+    vertex, moved inward along the vertex normal.  Returns a dict of float32
+    V, int32 F (global vertex indices), int32 face_body, float32 body_pos,
+    float32 S and int32 src_body."""
+    Vs, Fs, fb, pos, Ss, sb = [], [], [], [], [], []
+    off = 0
+    for b, (subdiv, axes, rv, p, depth) in enumerate(bodies):
+        V, F = icosphere_mesh(subdiv)
+        V = _f32((V * np.asarray(axes, np.float64)) @ rotvec_matrix(rv).T + np.asarray(p, np.float64))
+        Ss.append(_f32(V - depth * vertex_normals(V, F)))
+        Vs.append(V)
+        Fs.append(F + off)
+        off += V.shape[0]
+        fb.append(np.full(F.shape[0], b, np.int32))
+        sb.append(np.full(V.shape[0], b, np.int32))
+        pos.append(p)
+    return {"V": np.concatenate(Vs).astype(np.float32), "F": np.concatenate(Fs).astype(np.int32),
+            "face_body": np.concatenate(fb), "body_pos": _f32(np.array(pos)).astype(np.float32),
+            "S": np.concatenate(Ss).astype(np.float32), "src_body": np.concatenate(sb)}

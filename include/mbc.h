@@ -254,6 +254,27 @@ mbc_status mbc_mlp_train_step(mbc_mlp *net, int32_t batch, const float *X, const
 mbc_status mbc_warm_correct(int32_t n, int32_t R, const int32_t *src_body, int32_t n_bodies,
                             const float *U, const float *H, float *X, mbc_stream stream);
 
+/* Mesh collocation operator, assembled on the device: the collocation matrix
+ * of a triangle-mesh scene, the solid angle of every face seen from every
+ * source (utils/torch_utils.py:306-334, compute_solid_angle), and the
+ * rigid-mode right-hand side FL @ IQ (core/KTAB_Mfs_spclf1d.py:101-111 with
+ * utils/torch_utils.py:49-75), which the reference builds in torch each step:
+ *   M[f, j] = 2 atan2(R1.(R2 x R3), l1 l2 l3 + (R1.R2) l3 + (R1.R3) l2 + (R2.R3) l1),
+ *             Rk = V[F[f, k]] - S[j]          (n_faces x n_src, row stride ldm)
+ *   rhs[f, 6b .. 6b+5] = (s, r x s) for face f of body b, zero elsewhere
+ *             s = (v2 - v1) x (v3 - v1) / 2, r = face centre - body_pos[b]
+ *             (n_faces x 6 n_bodies; rhs NULL to skip)
+ * Computed in FP64 from float32 coordinates, stored as dtype (MBC_F32 for the
+ * mfs_torch operator, or MBC_F64).  V: device n_vert x 3; F: device n_faces x 3
+ * int32 vertex indices, counter-clockwise seen from outside; face_body: device
+ * int32[n_faces]; body_pos: device n_bodies x 3; S: device n_src x 3.  A face
+ * naming a vertex or body out of range gets NaN entries (nothing out of
+ * bounds is read). */
+mbc_status mbc_mesh_assemble(int32_t n_vert, const float *V, int32_t n_faces, const int32_t *F,
+                             const int32_t *face_body, int32_t n_bodies, const float *body_pos,
+                             int32_t n_src, const float *S, int32_t dtype, void *M, int64_t ldm,
+                             void *rhs, mbc_stream stream);
+
 /* Point-kernel matvec that allocates no device memory.  No counterpart in the
  * reference: it serves callers that cannot let a library call cudaMalloc or
  * cudaFree -- hosts that own the device through their own memory pool or a

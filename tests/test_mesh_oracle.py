@@ -46,3 +46,16 @@ def test_rhs_blocks_follow_the_bodies():
         b = z["face_body"][f]
         other = np.delete(rhs[f].reshape(-1, 6), b, axis=0)
         assert np.all(other == 0.0)
+
+
+FIXTURE_BODIES = [(1, (1.0, 0.7, 0.5), (0.3, -0.5, 0.2), (0.3, -0.2, 0.1), 0.1),
+                  (1, (0.6, 0.6, 0.6), (-0.4, 0.1, 0.7), (2.6, 0.4, -0.3), 0.08)]
+
+
+def test_mesh_scene_reproduces_fixture_inputs():
+    # the package's own vertex normals place the sources exactly where the
+    # reference's compute_normal_vertex put them for the fixture
+    z = np.load(GOLD)
+    m = S.mesh_scene(FIXTURE_BODIES)
+    for k in ("V", "F", "face_body", "body_pos", "S"):
+        assert np.array_equal(m[k], z[k]), k
