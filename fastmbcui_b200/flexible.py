@@ -21,20 +21,26 @@ def _colsum(a):
     return a.sum(dim=0)
 
 
-def flexible_cg(apply64, inner, b, tol=1e-8, keep=20, max_outer=300, check_true=True):
+def flexible_cg(apply64, inner, b, tol=1e-8, keep=20, max_outer=300, check_true=True, x0=None):
     """Solve A X = B column by column (batched), A symmetric positive definite.
 
     apply64(V) -> A V (FP64, n x R); inner(R) -> an approximation of A^-1 R for
-    columns scaled to unit norm.  Stops a column when |r| <= tol |b|; with
-    check_true the recursive residual is confirmed by b - A x before
-    stopping (and replaces r if it had drifted).  Returns (X, info)."""
+    columns scaled to unit norm.  x0: a starting point (costs one more FP64
+    application).  Stops a column when |r| <= tol |b|; with check_true the
+    recursive residual is confirmed by b - A x before stopping (and replaces r
+    if it had drifted).  Returns (X, info)."""
     import torch
 
-    x = torch.zeros_like(b)
-    r = b.clone()
+    n_apply, n_outer, n_replace = 0, 0, 0
+    if x0 is None:
+        x = torch.zeros_like(b)
+        r = b.clone()
+    else:
+        x = x0.to(b.dtype).clone()
+        r = b - apply64(x)
+        n_apply += 1
     bn = torch.linalg.norm(b, dim=0)
     P, Q, PQ = [], [], []
-    n_apply, n_outer, n_replace = 0, 0, 0
     for k in range(max_outer):
         rn = torch.linalg.norm(r, dim=0)
         done = rn <= tol * bn
@@ -79,13 +85,15 @@ def flexible_cg(apply64, inner, b, tol=1e-8, keep=20, max_outer=300, check_true=
                "relres_max": float(rel.max()), "converged": int((rel <= tol).sum())}
 
 
-def solve_flexible(s64, s32, F, tol=1e-8, inner_iters=40, keep=20, max_outer=300, adjoint=False):
+def solve_flexible(s64, s32, F, tol=1e-8, inner_iters=40, keep=20, max_outer=300, adjoint=False, X0=None):
     """Forward solve (K^T K) X = K^T F (or, with adjoint, (K^T K) X = F) with
     FP64 flexible CG around the FP32 solver's plain PCG.
 
-    s64, s32: solvers of the same plan and operator, precision FP64 and FP32,
-    both factored.  Returns (X float64, n x R, original order; info) where
-    info also counts the FP32 inner iterations."""
+    s64, s32: solvers of the same plan and operator, precision FP64 and FP32;
+    s32 factored (its KL factor preconditions the inner PCG), s64 used only
+    for operator applications.  X0: optional n x R start (original order).
+    Returns (X float64, n x R, original order; info) where info also counts
+    the FP32 inner iterations."""
     import torch
 
     F = F if F.dim() == 2 else F[:, None]
@@ -102,7 +110,8 @@ def solve_flexible(s64, s32, F, tol=1e-8, inner_iters=40, keep=20, max_outer=300
         counts["inner"] += int(st["iters_max"])
         return z.double()
 
-    X, info = flexible_cg(apply64, inner, b, tol=tol, keep=keep, max_outer=max_outer)
+    X, info = flexible_cg(apply64, inner, b, tol=tol, keep=keep, max_outer=max_outer,
+                          x0=None if X0 is None else X0.double())
     info["fp32_inner_iterations"] = counts["inner"]
     return X, info
 

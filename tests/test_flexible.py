@@ -94,3 +94,18 @@ def test_frozen_and_zero_columns(system):
     x, info = flexible_cg(apply64, inner, b3, tol=1e-8)
     assert torch.isfinite(x).all() and bool((x[:, 2] == 0).all())
     assert info["relres_max"] <= 1e-8
+
+
+def test_warm_start(system):
+    apply64, apply32, pcg, b = system
+
+    def inner(r):
+        return pcg(apply32, r, 30)[0]
+
+    x, cold = flexible_cg(apply64, inner, b, tol=1e-8)
+    # a start near the solution (as along a trajectory) takes fewer FP64 applications
+    x0 = x * (1 + 1e-3 * torch.randn(x.shape, dtype=x.dtype, generator=torch.Generator().manual_seed(0)))
+    x1, warm = flexible_cg(apply64, inner, b, tol=1e-8, x0=x0)
+    rel = torch.linalg.norm(b - apply64(x1), dim=0) / torch.linalg.norm(b, dim=0)
+    assert float(rel.max()) <= 1e-8
+    assert warm["fp64_applies"] < cold["fp64_applies"], (warm, cold)
