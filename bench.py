@@ -223,6 +223,20 @@ def run_trajectory(args):
         X0 = start(k, hist)
         s = F.Solver(plans[k], x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F32)
         s.set_matvec(MATVEC[args.matvec]).factor()
+        if args.solver == "flexible":
+            # FP64 flexible CG around the FP32 PCG; the FP64 solver only applies K
+            from fastmbcui_b200.flexible import solve_flexible
+
+            s64 = F.Solver(plans[k], x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64)
+            X, info = solve_flexible(s64, s, Fm[k], tol=1e-8, inner_iters=args.inner_iters, X0=X0,
+                                     profile=bool(profile))
+            st = {"iters_max": info["fp32_inner_iterations"], "iters_total": info["fp32_inner_iterations"] * R,
+                  "refinements": info["fp64_applies"], "n_polished": 0, "true_relres_max": info["relres_max"],
+                  "n_converged": info["converged"], "kernel_launches": info["kernel_launches"],
+                  "n_matvec": info["n_matvec64"] + info["n_matvec32"],
+                  "t_matvec_ms": info["t_matvec64_ms"] + info["t_matvec32_ms"],
+                  "n_matvec64": info["n_matvec64"], "t_matvec64_ms": info["t_matvec64_ms"]}
+            return X.float(), st
         X, st = s.solve(Fm[k], X0=X0, out_dtype=torch.float32, profile=profile, **opts)
         return X, st
 
@@ -308,12 +322,13 @@ def run_trajectory(args):
         "data": "synthetic (seeded trajectory)",
         "config": {"workload": "trajectory32", "desc": WORKLOADS["trajectory32"][1], "N": base.n,
                    "Nf": base.nf, "R": R, "rho": base.rho, "lambda": base.lam, "tol": 1e-8,
-                   "precision": "mixed FP32/FP64 residual replacement", "schedule": "batched",
+                   "precision": ("FP64 flexible CG around FP32 PCG" if args.solver == "flexible"
+                                 else "mixed FP32/FP64 residual replacement"), "schedule": "batched",
                    "warm_start": {"learned": "previous step + MLP correction (3x256, BF16 weights)",
                                   "extrapolate": "quadratic extrapolation of the last three steps' strengths",
                                   "previous": "previous step's strengths", "cold": "x0 = 0"}[args.warm],
                    "steps_run": f"{args.warmup} warm-up + {args.steps} timed",
-                   "plan_every": args.plan_every,
+                   "plan_every": args.plan_every, "solver": args.solver,
                    "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas{world}"},
         "e2e": {"value": round(e2e, 5), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h),
@@ -694,6 +709,9 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=572)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scenes", type=int, default=8, help="uneven workload: scenes in the sample")
+    ap.add_argument("--solver", default="mixed", choices=["mixed", "flexible"],
+                    help="trajectory: residual-replacement mixed PCG, or FP64 flexible CG around the FP32 PCG")
+    ap.add_argument("--inner-iters", type=int, default=40, help="flexible solver: FP32 iterations per outer step")
     ap.add_argument("--plan-every", type=int, default=1,
                     help="trajectory: rebuild the host plan every K steps (K > 1 reuses it, not the plain method)")
     ap.add_argument("--warm", default="extrapolate", choices=["extrapolate", "learned", "previous", "cold"],

@@ -85,34 +85,51 @@ def flexible_cg(apply64, inner, b, tol=1e-8, keep=20, max_outer=300, check_true=
                "relres_max": float(rel.max()), "converged": int((rel <= tol).sum())}
 
 
-def solve_flexible(s64, s32, F, tol=1e-8, inner_iters=40, keep=20, max_outer=300, adjoint=False, X0=None):
+def solve_flexible(s64, s32, F, tol=1e-8, inner_iters=40, keep=20, max_outer=300, adjoint=False, X0=None,
+                   profile=False):
     """Forward solve (K^T K) X = K^T F (or, with adjoint, (K^T K) X = F) with
     FP64 flexible CG around the FP32 solver's plain PCG.
 
     s64, s32: solvers of the same plan and operator, precision FP64 and FP32;
     s32 factored (its KL factor preconditions the inner PCG), s64 used only
     for operator applications.  X0: optional n x R start (original order).
-    Returns (X float64, n x R, original order; info) where info also counts
-    the FP32 inner iterations."""
+    Returns (X float64, n x R, original order; info).  info adds the FP32
+    inner iterations and library kernel launches and, with profile, the
+    CUDA-event time of the FP64 applications and of the inner matvecs."""
     import torch
 
     F = F if F.dim() == 2 else F[:, None]
     F64 = F.double().contiguous()
     b = F64 if adjoint else s64.apply_KT(F64)
-    counts = {"inner": 0}
+    acc = {"inner": 0, "launches": 2 if not adjoint else 0, "t64": 0.0, "n64": 0, "t32": 0.0, "n32": 0}
 
     def apply64(v):
-        return s64.apply_KT(s64.apply_K(v.contiguous()))
+        if profile:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+        out = s64.apply_KT(s64.apply_K(v.contiguous()))
+        if profile:
+            e1.record()
+            e1.synchronize()
+            acc["t64"] += e0.elapsed_time(e1)
+        acc["n64"] += 2
+        acc["launches"] += 4  # permute, K, K^T, permute
+        return out
 
     def inner(rs):
         z, st = s32.solve_adjoint(rs.float().contiguous(), out_dtype=torch.float32, tol=0.0,
-                                  max_iters=inner_iters, max_refine=0)
-        counts["inner"] += int(st["iters_max"])
+                                  max_iters=inner_iters, max_refine=0, profile=1 if profile else 0)
+        acc["inner"] += int(st["iters_max"])
+        acc["launches"] += int(st["kernel_launches"])
+        acc["t32"] += float(st["t_matvec_ms"])
+        acc["n32"] += int(st["n_matvec"])
         return z.double()
 
     X, info = flexible_cg(apply64, inner, b, tol=tol, keep=keep, max_outer=max_outer,
                           x0=None if X0 is None else X0.double())
-    info["fp32_inner_iterations"] = counts["inner"]
+    info.update({"fp32_inner_iterations": acc["inner"], "kernel_launches": acc["launches"],
+                 "t_matvec64_ms": acc["t64"], "n_matvec64": acc["n64"], "t_matvec32_ms": acc["t32"],
+                 "n_matvec32": acc["n32"]})
     return X, info
 
 
