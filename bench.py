@@ -222,12 +222,13 @@ def run_trajectory(args):
         x, nx, y = coords[k]
         X0 = start(k, hist)
         s = F.Solver(plans[k], x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F32)
-        s.set_matvec(MATVEC[args.matvec]).factor()
+        s.set_matvec(MATVEC[args.matvec]).set_fp64_matvec(args.fp64_matvec).factor()
         if args.solver == "flexible":
             # FP64 flexible CG around the FP32 PCG; the FP64 solver only applies K
             from fastmbcui_b200.flexible import solve_flexible
 
             s64 = F.Solver(plans[k], x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64)
+            s64.set_fp64_matvec(args.fp64_matvec)
             X, info = solve_flexible(s64, s, Fm[k], tol=1e-8, inner_iters=args.inner_iters, X0=X0,
                                      profile=bool(profile))
             st = {"iters_max": info["fp32_inner_iterations"], "iters_total": info["fp32_inner_iterations"] * R,
@@ -314,7 +315,7 @@ def run_trajectory(args):
     del plain
 
     st = stats[-1]
-    roofline = _matvec_roofline(st, scenes[0].nf, scenes[0].n, R, args.matvec)
+    roofline = _matvec_roofline(st, scenes[0].nf, scenes[0].n, R, args.matvec, args.fp64_matvec)
     out = {
         "metric": METRIC, "value": round(value, 5), "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
@@ -328,7 +329,7 @@ def run_trajectory(args):
                                   "extrapolate": "quadratic extrapolation of the last three steps' strengths",
                                   "previous": "previous step's strengths", "cold": "x0 = 0"}[args.warm],
                    "steps_run": f"{args.warmup} warm-up + {args.steps} timed",
-                   "plan_every": args.plan_every, "solver": args.solver,
+                   "plan_every": args.plan_every, "solver": args.solver, "fp64_matvec": args.fp64_matvec,
                    "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas{world}"},
         "e2e": {"value": round(e2e, 5), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h),
@@ -362,11 +363,15 @@ def run_trajectory(args):
 TC_TRAFFIC_BYTES = 442e6
 
 
-def _matvec_roofline(st, nf, n, R, matvec):
+def _matvec_roofline(st, nf, n, R, matvec, fp64_matvec="simt"):
     """Roofline of the dominant kernel of the timed solve, from live CUDA
     events: the K / K^T matvec pairs, split by precision.  Algorithmic work
     per launch: nf * n * (20 + 2 R) flops (R = the columns the launch carries:
-    all R for the FP32 recursion, the polished columns for FP64)."""
+    all R for the FP32 recursion, the polished columns for FP64).  The INT8
+    form of the FP64 matvec is rated on its own work instead: 15 digit-plane
+    products, 2 * 15 * nf * n * R integer ops, against twice the measured
+    dense BF16 rate (the nominal INT8 : BF16 ratio), and on its HBM stream,
+    5 bytes of digit planes per matrix entry."""
     hbm, bf16, src = _peaks()
     n64, t64 = st.get("n_matvec64", 0), st.get("t_matvec64_ms", 0.0)
     n32, t32 = st["n_matvec"] - n64, st["t_matvec_ms"] - t64
@@ -388,6 +393,25 @@ def _matvec_roofline(st, nf, n, R, matvec):
             "launches": int(n64), "columns": R64, "achieved_tflops": round(a64, 2), "total_ms": round(t64, 1),
             "fp64_nominal_tflops": 37.0, "frac_of_fp64_nominal": round(a64 / 37.0, 4)}
     dom64 = t64 >= t32
+    if fp64_matvec == "int8":
+        # per launch (one direction): pack + MMA kernel
+        sec = ms64 * 1e-3 if n64 else float("inf")
+        tops = 2.0 * 15 * nf * n * R64 / sec / 1e12
+        gbs = 5.0 * nf * n / sec / 1e9
+        fp64.update({"kernel": "oz_pack_b_kernel + oz_mma_kernel (tcgen05 kind::i8, 5-digit slicing)",
+                     "achieved_int8_tops": round(tops, 1), "int8_peak_tops": 2 * bf16,
+                     "frac_of_int8": round(tops / (2 * bf16), 4), "plane_gbs": round(gbs, 1),
+                     "frac_of_hbm": round(gbs / hbm, 4)})
+        if dom64:
+            tensor_side = tops / (2 * bf16) >= gbs / hbm
+            return {"bound": "tensor" if tensor_side else "hbm",
+                    "achieved": round(tops if tensor_side else gbs, 2),
+                    "peak": 2 * bf16 if tensor_side else hbm, "unit": "TOPS" if tensor_side else "GB/s",
+                    "frac": round(tops / (2 * bf16) if tensor_side else gbs / hbm, 4), "traffic": None,
+                    "kernel": fp64["kernel"], "launch_ms": round(ms64, 3),
+                    "peak_source": f"INT8 dense = 2 x bf16 dense, {src} (derived from measured); "
+                                   f"HBM {hbm} GB/s (of measured)",
+                    "fp64_matvec": fp64, "tensor_matvec": tc}
     ach, ms = (a64, ms64) if dom64 else (a32, ms32)
     return {"bound": "tensor", "achieved": round(ach, 2), "peak": bf16, "unit": "TFLOP/s",
             "frac": round(ach / bf16, 4), "traffic": None if dom64 else tc["traffic"],
@@ -462,7 +486,7 @@ def run_ours(args):
     t_plan = time.perf_counter() - t0
     x, nx, y, Fd = t(sc.x), t(sc.nx), t(sc.y), t(Fm)
     solver = F.Solver(plan, x=x, nx=nx, y=y, coef=sc.coef, precision=F.MBC_F32)
-    solver.set_matvec(MATVEC[args.matvec])
+    solver.set_matvec(MATVEC[args.matvec]).set_fp64_matvec(args.fp64_matvec)
     opts = dict(tol=1e-8, max_iters=args.max_iters, max_refine=64, inner_tol=1e-2, check_every=8)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
 
@@ -533,7 +557,7 @@ def run_ours(args):
     plain_sps = 1000.0 / _max_over_ranks(dist, plain_ms)
 
     st = stats[-1]
-    roofline = _matvec_roofline(st, sc.nf, sc.n, R, args.matvec)
+    roofline = _matvec_roofline(st, sc.nf, sc.n, R, args.matvec, args.fp64_matvec)
     out = {
         "metric": METRIC, "value": round(value, 5), "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
@@ -627,7 +651,7 @@ def run_probe(args):
     f64 = args.probe_precision == "f64"
     solver = F.Solver(plan, x=t(sc.x), nx=t(sc.nx), y=t(sc.y), coef=sc.coef,
                       precision=F.MBC_F64 if f64 else F.MBC_F32)
-    solver.set_matvec(MATVEC[args.matvec]).factor()
+    solver.set_matvec(MATVEC[args.matvec]).set_fp64_matvec(args.fp64_matvec).factor()
     if args.probe_solve:
         # one complete mixed solve (the launch list of a step)
         Fm = t(sc.rhs())
@@ -726,6 +750,8 @@ def main():
                     help="with --kernel-probe: one full mixed solve instead of K / K^T launches")
     ap.add_argument("--matvec", default="auto", choices=sorted(MATVEC),
                     help="FP32 matvec: tensor cores (3xTF32 tcgen05) or CUDA cores")
+    ap.add_argument("--fp64-matvec", default="simt", choices=["simt", "int8"],
+                    help="FP64 matvec: CUDA-core FP64 kernels or exact INT8 digit slicing on the tensor cores")
     args = ap.parse_args()
     if args.kernel_probe:
         run_probe(args)

@@ -11,12 +11,14 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import (MBC_F32, MBC_F64, MBC_MATVEC_AUTO, MBC_MATVEC_SIMT, MBC_MATVEC_TENSOR,
+from ._lib import (MBC_F32, MBC_F64, MBC_FP64_MATVEC_INT8, MBC_FP64_MATVEC_SIMT, MBC_MATVEC_AUTO,
+                   MBC_MATVEC_SIMT, MBC_MATVEC_TENSOR,
                    MBC_OP_DENSE, MBC_OP_POINT_KERNEL, MBC_SCHED_BATCHED, MBC_SCHED_PER_RHS, MbcError,
                    check, ptr)
 
 __all__ = ["Plan", "Solver", "MbcError", "load", "MBC_F32", "MBC_F64", "MBC_SCHED_BATCHED",
-           "MBC_SCHED_PER_RHS", "MBC_MATVEC_AUTO", "MBC_MATVEC_SIMT", "MBC_MATVEC_TENSOR"]
+           "MBC_SCHED_PER_RHS", "MBC_MATVEC_AUTO", "MBC_MATVEC_SIMT", "MBC_MATVEC_TENSOR",
+           "MBC_FP64_MATVEC_SIMT", "MBC_FP64_MATVEC_INT8"]
 
 
 def load():
@@ -141,6 +143,20 @@ class Solver:
     def set_matvec(self, impl: int):
         """MBC_MATVEC_AUTO / _SIMT / _TENSOR (FP32 point-kernel solvers)."""
         check(load().mbc_solver_set_matvec(self._h, int(impl)), "mbc_solver_set_matvec")
+        return self
+
+    def set_fp64_matvec(self, impl):
+        """How the FP64 matvecs run (mbc_solver_set_fp64_matvec): "simt"
+        (MBC_FP64_MATVEC_SIMT, the default) or "int8" (MBC_FP64_MATVEC_INT8,
+        exact digit slicing on the INT8 tensor cores, 10 bytes of device
+        memory per matrix entry)."""
+        impl = {"simt": MBC_FP64_MATVEC_SIMT, "int8": MBC_FP64_MATVEC_INT8}.get(impl, impl)
+        check(load().mbc_solver_set_fp64_matvec(self._h, int(impl)), "mbc_solver_set_fp64_matvec")
+        return self
+
+    def prepare(self):
+        """Build what the selected matvecs need now (mbc_solver_prepare)."""
+        check(load().mbc_solver_prepare(self._h, self._sp()), "mbc_solver_prepare")
         return self
 
     def pivot_retries(self) -> int:

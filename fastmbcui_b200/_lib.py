@@ -20,6 +20,7 @@ MBC_F64, MBC_F32 = 0, 1
 MBC_OP_DENSE, MBC_OP_POINT_KERNEL = 0, 1
 MBC_SCHED_BATCHED, MBC_SCHED_PER_RHS = 0, 1
 MBC_MATVEC_AUTO, MBC_MATVEC_SIMT, MBC_MATVEC_TENSOR = 0, 1, 2
+MBC_FP64_MATVEC_SIMT, MBC_FP64_MATVEC_INT8 = 0, 1
 
 
 class PlanOptions(C.Structure):
@@ -79,6 +80,8 @@ SIGNATURES = {
     "mbc_solver_get_factor": (C.c_int, [_vp, _vp, _vp]),
     "mbc_solver_get_pivot_retries": (C.c_int, [_vp, C.POINTER(_i32)]),
     "mbc_solver_set_matvec": (C.c_int, [_vp, _i32]),
+    "mbc_solver_set_fp64_matvec": (C.c_int, [_vp, _i32]),
+    "mbc_solver_prepare": (C.c_int, [_vp, _vp]),
     "mbc_solve_default_options": (None, [C.POINTER(SolveOptions)]),
     "mbc_solve": (C.c_int, [_vp, _i32, _vp, _i32, _vp, _i32, _vp, C.POINTER(SolveOptions),
                             C.POINTER(SolveStats), _vp, _vp]),

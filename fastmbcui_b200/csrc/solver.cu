@@ -16,6 +16,7 @@
 #include "forces.cuh"
 #include "matvec.cuh"
 #include "matvec_tc.cuh"
+#include "matvec_oz.cuh"
 #include "mbc_internal.h"
 #include "pcg.cuh"
 #include "solver.h"
@@ -213,6 +214,68 @@ static int tc_launch(const Solver &S, int R, const float *vin, float *out, const
   return (int)grid;
 }
 
+// FP64-accurate INT8 path: an FP64 point-kernel matvec once the digit
+// planes of G are built (Solver::ensure_oz)
+static bool use_oz(const Solver &S)
+{
+  return S.fp64_matvec == MBC_FP64_MATVEC_INT8 && S.oz_ready && S.op.kind == MBC_OP_POINT_KERNEL;
+}
+
+template <int NPH>
+static void oz_mma_launch(const oz::OzArgs &a, unsigned grid, cudaStream_t st)
+{
+  oz::oz_mma_kernel<NPH><<<grid, oz::kThreads, oz::smem_bytes(2 * NPH), st>>>(a);
+}
+
+template <int NPH>
+static mbc_status oz_allow()
+{
+  return allow_max_smem(oz::oz_mma_kernel<NPH>, oz::smem_bytes(2 * NPH));
+}
+
+// pack the vector block, then the MMA kernel; returns the row tiles (the
+// rows of the curvature partials), 0 if the buffers were not prepared
+template <int DIR>
+static int oz_launch(const Solver &S, int R, const double *vin, double *out, const double *pdot,
+                     double *part, const int32_t *done, cudaStream_t st)
+{
+  const int M = DIR == 0 ? S.nf : S.n;
+  const int K = DIR == 0 ? S.n : S.nf;
+  const int np = oz::np_for(R), groups = oz::groups_for(R);
+  if (S.m_oz_b.bytes < oz::bimg_bytes(K, R) || S.m_oz_bexp.bytes < sizeof(int32_t) * oz::bexp_count(K, R)) {
+    S.oz_unprepared = true;
+    return 0;
+  }
+  oz::oz_pack_b_kernel<<<dim3(oz::nchunks_for(K), groups), 512, 0, st>>>(
+      vin, K, R, np, (int8_t *)S.m_oz_b.ptr, (int32_t *)S.m_oz_bexp.ptr, done);
+  oz::OzArgs a{};
+  a.adig = (const int8_t *)S.m_oz_a[DIR].ptr;
+  a.aexp = (const int32_t *)S.m_oz_aexp[DIR].ptr;
+  a.bimg = (const int8_t *)S.m_oz_b.ptr;
+  a.bexp = (const int32_t *)S.m_oz_bexp.ptr;
+  a.out = out;
+  a.M = M;
+  a.K = K;
+  a.R = R;
+  a.groups = groups;
+  a.coef = S.op.coef;
+  a.pdot = pdot;
+  a.part = part;
+  a.done = done;
+  a.err = (int32_t *)S.m_err.ptr;
+  const unsigned grid = (unsigned)oz::row_tiles(M) * (unsigned)groups;
+  switch (np) {
+    case 16: oz_mma_launch<8>(a, grid, st); break;
+    case 32: oz_mma_launch<16>(a, grid, st); break;
+    case 48: oz_mma_launch<24>(a, grid, st); break;
+    case 64: oz_mma_launch<32>(a, grid, st); break;
+    case 80: oz_mma_launch<40>(a, grid, st); break;
+    default: oz_mma_launch<48>(a, grid, st); break;
+  }
+  S.launches += 2;
+  return oz::row_tiles(M);
+}
+
 #define MBC_SHAPES(T, X)                                                   \
   X(T, 1, 64) X(T, 1, 128) X(T, 4, 64) X(T, 8, 64) X(T, 16, 64) X(T, 32, 64) X(T, 32, 128)
 
@@ -222,9 +285,16 @@ void launch_rows(const Solver &S, int R, const T *v, T *w, const int32_t *done, 
   if constexpr (sizeof(T) == 4) {
     if (use_tc(S, R)) {
       tc_launch<0>(S, R, v, w, nullptr, nullptr, done, st);
+      S.launches += 2;
+      return;
+    }
+  } else {
+    if (use_oz(S)) {
+      oz_launch<0>(S, R, v, w, nullptr, nullptr, done, st);
       return;
     }
   }
+  ++S.launches;
   const Shape sh = pick_shape<T>(S.op.kind == MBC_OP_POINT_KERNEL ? S.nf : 1 << 30, R);
 #define MBC_ROWS_CASE(TT, RC_, TI_) \
   if (sh.rc == RC_ && sh.ti == TI_) return rows_launch<T, RC_, TI_>(S, R, v, w, done, st);
@@ -241,8 +311,14 @@ int launch_cols(const Solver &S, int R, const T *w, T *t, const T *pdot, double 
                 const int32_t *done, cudaStream_t st)
 {
   if constexpr (sizeof(T) == 4) {
-    if (use_tc(S, R)) return tc_launch<1>(S, R, w, t, pdot, part, done, st);
+    if (use_tc(S, R)) {
+      S.launches += 2;
+      return tc_launch<1>(S, R, w, t, pdot, part, done, st);
+    }
+  } else {
+    if (use_oz(S)) return oz_launch<1>(S, R, w, t, pdot, part, done, st);
   }
+  ++S.launches;
   const Shape sh = pick_shape<T>(S.n, R);
 #define MBC_COLS_CASE(TT, RC_, TI_) \
   if (sh.rc == RC_ && sh.ti == TI_) return cols_launch<T, RC_, TI_>(S, R, w, t, pdot, part, done, st);
@@ -655,7 +731,7 @@ static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, XT *x, const LT *lval
       update_xr_kernel<T, XT><<<L.grid, L.block, L.smem, st>>>(S.n, R, w.sc.alpha, w.Pv, w.Tt, x,
                                                                w.Rv, w.part, w.sc.done);
       reduce_kernel<<<1, 1024, 0, st>>>(nblk2, R, w.part, RED_CHECK, w.sc, nullptr);
-      S.launches += precond ? 9 : 8;
+      S.launches += precond ? 7 : 6;  // the matvec pair counts itself
     }
     if (use_graph && !graph.exec) {
       cudaGraph_t g = nullptr;
@@ -702,7 +778,7 @@ static void residual(Solver &S, int R, const T *F, const T *X, T *W, T *Rout, cu
   const int64_t cnt = (int64_t)S.nf * R;
   sub_kernel<T><<<cdiv(cnt, 256), 256, 0, st>>>(cnt, F, W, W);
   launch_cols<T>(S, R, W, Rout, nullptr, nullptr, nullptr, st);
-  S.launches += 3;
+  ++S.launches;
 }
 
 // per-column norms^2 of an n x R array into host vector
@@ -825,11 +901,16 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
 {
   PcgWork<T> w;
   MBC_TRY(pcg_buffers<T>(*this, R, w));
-  // F (forward) lives in fbuf (T, nf x R)
+  // F (forward) lives in fbuf (T, nf x R); with the INT8 FP64 operator the
+  // adjoint right-hand side b is kept there too (n x R), for the replacements
   DevMem &fm = sizeof(T) == 8 ? fbuf64 : fbuf32;
+  const bool oz = sizeof(T) == 8 && use_oz(*this);
   if (!adjoint) {
     MBC_TRY(fm.reserve(sizeof(T) * (size_t)nf * R));
     load_rows<T>(*this, R, rhs, rhs_dt, (T *)fm.ptr, st);
+  } else if (oz) {
+    MBC_TRY(fm.reserve(sizeof(T) * (size_t)n * R));
+    permute_in<T>(*this, R, rhs, rhs_dt, (T *)fm.ptr, st);
   }
   const int64_t nv = (int64_t)n * R;
   if (X0) {
@@ -859,10 +940,31 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
     MBC_TRY(col_norms2_dev<T>(*this, R, bvec, (double *)b2ref.ptr, st));
     b2 = (const double *)b2ref.ptr;
   }
+  // The INT8 FP64 operator carries a ~1e-10 relative error, so the recursive
+  // residual drifts from b - K^T K x by about that much per hundred
+  // iterations: columns converge only on residuals recomputed with the same
+  // operator (replacement mode), which keeps p and the Krylov information.
+  std::function<mbc_status()> replace_fn = [&]() -> mbc_status {
+    const Layout2D L = layout2d(n, R);
+    if (adjoint) {
+      launch_rows<T>(*this, R, w.X, w.W, nullptr, st);
+      launch_cols<T>(*this, R, w.W, w.Tt, nullptr, nullptr, nullptr, st);
+      sub_kernel<T><<<cdiv(nv, 256), 256, 0, st>>>(nv, (const T *)fm.ptr, w.Tt, w.Rv);
+      ++launches;
+    } else {
+      residual<T>(*this, R, (const T *)fm.ptr, w.X, w.W, w.Rv, st);
+    }
+    dot_partial_kernel<T><<<L.grid, L.block, L.smem, st>>>(n, R, w.Rv, w.Rv, w.part);
+    reduce_kernel<<<1, 1024, 0, st>>>((int)L.grid.x, R, w.part, RED_REPLACE, w.sc, nullptr);
+    launches += 2;
+    MBC_CKL();
+    return MBC_OK;
+  };
+  if (oz) w.sc.drop2 = 1e-300;  // replace only where a column would stop
   if (precision == MBC_F64)
     MBC_TRY((run_pcg<T, double, T>(*this, R, w, w.X, (const double *)lval.ptr, o.max_iters, o.tol,
                                    o.precondition != 0, std::max(1, o.check_every), nullptr, st, b2,
-                                   nullptr, 0)));
+                                   oz ? &replace_fn : nullptr, oz ? 64 : 0)));
   else
     MBC_TRY((run_pcg<T, float, T>(*this, R, w, w.X, (const float *)lval.ptr, o.max_iters, o.tol,
                                   o.precondition != 0, std::max(1, o.check_every), nullptr, st, b2,
@@ -870,6 +972,8 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
   std::vector<int32_t> status, iters;
   std::vector<double> rel;
   MBC_TRY(collect<T>(*this, R, w, status, iters, rel, st));
+  for (int c = 0; c < R; ++c)
+    if (status[c] == COL_STAGNANT) status[c] = COL_MAXIT;
   permute_out<T>(*this, R, w.X, X, x_dt, st);
   MBC_CKL();
   MBC_TRY(finish_stats(R, status, iters, rel, stats, iters_host));
@@ -885,6 +989,13 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
 mbc_status Solver::true_residual(int R, const void *F, int32_t f_dt, const void *X, int32_t x_dt,
                                  mbc_solve_stats *stats, cudaStream_t st)
 {
+  // always the FP64 CUDA-core kernels, whatever FP64 matvec the solves use
+  struct Restore {
+    Solver &S;
+    int32_t impl;
+    ~Restore() { S.fp64_matvec = impl; }
+  } restore{*this, fp64_matvec};
+  fp64_matvec = MBC_FP64_MATVEC_SIMT;
   MBC_TRY(fbuf64.reserve(sizeof(double) * (size_t)nf * R));
   MBC_TRY(res64.reserve(sizeof(double) * ((size_t)nf * R + 2 * (size_t)n * R)));
   double *Fd = (double *)fbuf64.ptr;
@@ -929,7 +1040,6 @@ mbc_status Solver::solve_mixed(int R, const void *rhs, int32_t rhs_dt, void *X, 
   else {
     load_rows<double>(*this, R, rhs, rhs_dt, Fd, st);
     launch_cols<double>(*this, R, Fd, Bd, nullptr, nullptr, nullptr, st);
-    ++launches;
   }
   if (X0) permute_in<double>(*this, R, X0, x_dt, Xd, st);
   else MBC_CK(cudaMemsetAsync(Xd, 0, sizeof(double) * nv, st));
@@ -943,7 +1053,7 @@ mbc_status Solver::solve_mixed(int R, const void *rhs, int32_t rhs_dt, void *X, 
       launch_rows<double>(*this, R, Xd, Wd, nullptr, st);
       launch_cols<double>(*this, R, Wd, Rd, nullptr, nullptr, nullptr, st);
       sub_kernel<double><<<cdiv(nv, 256), 256, 0, st>>>(nv, Bd, Rd, Rd);
-      launches += 3;
+      ++launches;
     } else {
       residual<double>(*this, R, Fd, Xd, Wd, Rd, st);
     }
@@ -986,7 +1096,12 @@ mbc_status Solver::solve_mixed(int R, const void *rhs, int32_t rhs_dt, void *X, 
   std::vector<int32_t> pol;
   for (int c = 0; c < R; ++c)
     if (status[c] == COL_STAGNANT || status[c] == COL_MAXIT) pol.push_back(c);
-  if (!pol.empty()) {
+  const int32_t n_polished = (int32_t)pol.size();
+  // With the INT8 FP64 operator a polish run stops on its recursive
+  // residual, which can end just above tol once recomputed: such columns are
+  // polished again from where they stand (at most twice more).
+  const int passes = use_oz(*this) ? 3 : 1;
+  for (int pass = 0; pass < passes && !pol.empty(); ++pass) {
     const int Rs = (int)pol.size();
     MBC_TRY(polish_idx.reserve(sizeof(int32_t) * (Rs + 2) + sizeof(double) * R));
     int32_t *d_idx = (int32_t *)polish_idx.ptr;
@@ -1020,10 +1135,13 @@ mbc_status Solver::solve_mixed(int R, const void *rhs, int32_t rhs_dt, void *X, 
     std::vector<double> nr, nb;
     MBC_TRY(col_norms2<double>(*this, R, Rd, nr, st));
     MBC_TRY(col_norms2<double>(*this, R, Bd, nb, st));
+    std::vector<int32_t> again;
     for (int c : pol) {
       rel[c] = nb[c] < 1e-16 ? 0.0 : std::sqrt(nr[c] / nb[c]);
       status[c] = rel[c] <= o.tol ? COL_OK : COL_MAXIT;
+      if (status[c] != COL_OK) again.push_back(c);
     }
+    pol.swap(again);
   }
   permute_out<double>(*this, R, Xd, X, x_dt, st);
   MBC_CKL();
@@ -1031,7 +1149,7 @@ mbc_status Solver::solve_mixed(int R, const void *rhs, int32_t rhs_dt, void *X, 
     if (status[c] == COL_STAGNANT) status[c] = COL_MAXIT;
   MBC_TRY(finish_stats(R, status, iters, rel, stats, iters_host));
   if (stats) {
-    stats->n_polished = (int32_t)pol.size();
+    stats->n_polished = n_polished;
     stats->refinements = n_repl + 1;
     double m = 0;
     for (int c = 0; c < R; ++c) m = std::max(m, rel[c]);
@@ -1052,6 +1170,8 @@ mbc_status Solver::solve(int R, const void *rhs, int32_t rhs_dt, void *X, int32_
                          int32_t *iters_host, cudaStream_t st)
 {
   if (!factored) return fail(MBC_BAD_ARG, "solver is not factored (call mbc_solver_factor)");
+  MBC_TRY(ensure_oz(st, R));
+  oz_unprepared = false;
   const auto t0 = std::chrono::steady_clock::now();
   const int64_t launches0 = launches;
   profile = o.profile != 0;
@@ -1192,14 +1312,59 @@ mbc::Solver::~Solver()
 
 mbc_status mbc::Solver::check_device_error(cudaStream_t st)
 {
+  if (oz_unprepared) {
+    oz_unprepared = false;
+    return fail(MBC_CUDA_ERROR, "an INT8 matvec found its buffers unsized and did not run");
+  }
   int32_t e = 0;
   MBC_CK(cudaMemcpyAsync(&e, m_err.ptr, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   MBC_CK(cudaStreamSynchronize(st));
   if (e) {
     MBC_CK(cudaMemsetAsync(m_err.ptr, 0, sizeof(int32_t), st));
     if (e == 2) return fail(MBC_CUDA_ERROR, "tensor-core matvec: shared memory window not 1024-byte aligned");
+    if (e == 3) return fail(MBC_BAD_ARG, "non-finite kernel value: a source coincides with a collocation point");
     return fail(MBC_TIMEOUT, "a bounded device wait expired in the tensor-core matvec");
   }
+  return MBC_OK;
+}
+
+mbc_status mbc::Solver::ensure_oz(cudaStream_t st, int R)
+{
+  namespace oz = mbc::oz;
+  if (fp64_matvec != MBC_FP64_MATVEC_INT8) return MBC_OK;
+  if (op.kind != MBC_OP_POINT_KERNEL) return fail(MBC_UNSUPPORTED, "the INT8 FP64 matvec needs a point-kernel operator");
+  if (!oz_ready) {
+    const size_t a0 = oz::adig_bytes(nf, n), a1 = oz::adig_bytes(n, nf);
+    size_t free_b = 0, total_b = 0;
+    MBC_CK(cudaMemGetInfo(&free_b, &total_b));
+    if (a0 + a1 + ((size_t)1 << 30) > free_b)
+      return fail(MBC_NO_MEMORY, "INT8 matvec digit planes need " + std::to_string((a0 + a1) >> 20) + " MiB, " +
+                                     std::to_string(free_b >> 20) + " MiB free");
+    MBC_TRY(m_oz_a[0].reserve(a0));
+    MBC_TRY(m_oz_a[1].reserve(a1));
+    MBC_TRY(m_oz_aexp[0].reserve(sizeof(int32_t) * oz::aexp_count(nf, n)));
+    MBC_TRY(m_oz_aexp[1].reserve(sizeof(int32_t) * oz::aexp_count(n, nf)));
+    const size_t sm0 = sizeof(float4) * oz::kChunk, sm1 = 2 * sizeof(float4) * oz::kChunk;
+    MBC_TRY(allow_max_smem(oz::oz_digits_kernel<0>, sm0));
+    MBC_TRY(allow_max_smem(oz::oz_digits_kernel<1>, sm1));
+    MBC_TRY(oz_allow<8>());
+    MBC_TRY(oz_allow<16>());
+    MBC_TRY(oz_allow<24>());
+    MBC_TRY(oz_allow<32>());
+    MBC_TRY(oz_allow<40>());
+    MBC_TRY(oz_allow<48>());
+    oz::oz_digits_kernel<0><<<dim3(oz::nchunks_for(n), oz::row_tiles(nf)), 256, sm0, st>>>(
+        x4(), n4(), y4(), nf, n, (int8_t *)m_oz_a[0].ptr, (int32_t *)m_oz_aexp[0].ptr, (int32_t *)m_err.ptr);
+    oz::oz_digits_kernel<1><<<dim3(oz::nchunks_for(nf), oz::row_tiles(n)), 256, sm1, st>>>(
+        x4(), n4(), y4(), nf, n, (int8_t *)m_oz_a[1].ptr, (int32_t *)m_oz_aexp[1].ptr, (int32_t *)m_err.ptr);
+    launches += 2;
+    MBC_CKL();
+    MBC_TRY(check_device_error(st));
+    oz_ready = true;
+  }
+  const int K = std::max(n, nf);
+  MBC_TRY(m_oz_b.reserve(oz::bimg_bytes(K, R)));
+  MBC_TRY(m_oz_bexp.reserve(sizeof(int32_t) * oz::bexp_count(K, R)));
   return MBC_OK;
 }
 
@@ -1262,6 +1427,24 @@ extern "C" mbc_status mbc_solver_set_matvec(mbc_solver *s, int32_t impl)
   return MBC_OK;
 }
 
+extern "C" mbc_status mbc_solver_set_fp64_matvec(mbc_solver *s, int32_t impl)
+{
+  if (!s) return fail(MBC_BAD_ARG, "NULL solver");
+  if (impl != MBC_FP64_MATVEC_SIMT && impl != MBC_FP64_MATVEC_INT8) return fail(MBC_BAD_ARG, "unknown FP64 matvec implementation");
+  if (impl == MBC_FP64_MATVEC_INT8 && s->s.op.kind != MBC_OP_POINT_KERNEL)
+    return fail(MBC_UNSUPPORTED, "the INT8 FP64 matvec needs a point-kernel operator");
+  s->s.fp64_matvec = impl;
+  return MBC_OK;
+}
+
+extern "C" mbc_status mbc_solver_prepare(mbc_solver *s, mbc_stream stream)
+{
+  if (!s) return fail(MBC_BAD_ARG, "NULL solver");
+  MBC_TRY(s->s.ensure_oz((cudaStream_t)stream, 1));
+  MBC_CK(cudaStreamSynchronize((cudaStream_t)stream));
+  return MBC_OK;
+}
+
 extern "C" void mbc_solve_default_options(mbc_solve_options *o)
 {
   if (!o) return;
@@ -1317,6 +1500,7 @@ extern "C" mbc_status mbc_apply_K(mbc_solver *s, int32_t R, const void *V, void 
   mbc::Solver &S = s->s;
   cudaStream_t st = (cudaStream_t)stream;
   if (S.precision == MBC_F64) {
+    MBC_TRY(S.ensure_oz(st, R));
     MBC_TRY(S.tmp.reserve(sizeof(double) * (size_t)S.n * R));
     mbc::permute_in<double>(S, R, V, MBC_F64, (double *)S.tmp.ptr, st);
     mbc::launch_rows<double>(S, R, (const double *)S.tmp.ptr, (double *)W, nullptr, st);
@@ -1335,6 +1519,7 @@ extern "C" mbc_status mbc_apply_KT(mbc_solver *s, int32_t R, const void *W, void
   mbc::Solver &S = s->s;
   cudaStream_t st = (cudaStream_t)stream;
   if (S.precision == MBC_F64) {
+    MBC_TRY(S.ensure_oz(st, R));
     MBC_TRY(S.tmp.reserve(sizeof(double) * (size_t)S.n * R));
     mbc::launch_cols<double>(S, R, (const double *)W, (double *)S.tmp.ptr, nullptr, nullptr, nullptr, st);
     mbc::permute_out<double>(S, R, (const double *)S.tmp.ptr, T, MBC_F64, st);

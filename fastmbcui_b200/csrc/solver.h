@@ -29,11 +29,14 @@ struct Solver {
   bool factored = false;
   int32_t pivot_retries = 0;
   int32_t *h_flag = nullptr;  // pinned
-  int64_t launches = 0;       // kernels launched by this solver (solve paths)
+  mutable int64_t launches = 0;  // kernels launched by this solver
   int32_t replacements = 0;   // residual replacements in the last PCG run
   bool profile = false;
   bool graph = false;  // replay PCG iteration blocks as CUDA graphs
   int32_t matvec_impl = MBC_MATVEC_AUTO;
+  int32_t fp64_matvec = MBC_FP64_MATVEC_SIMT;
+  bool oz_ready = false;  // INT8 digit planes of G built for the current geometry
+  mutable bool oz_unprepared = false;  // an INT8 launch found its buffers unsized (not run)
   std::vector<cudaEvent_t> events;
   std::vector<float> prof_ms_all;
   std::vector<int> prof_is64;  // 1: the pair ran in FP64
@@ -46,6 +49,10 @@ struct Solver {
   DevMem m_x4, m_n4, m_y4;
   DevMem m_err;           // set by a tensor-core kernel (1: a bounded wait expired)
   mutable DevMem m_bimg;  // packed TF32 hi/lo image of the tensor-core B operand
+  // FP64-accurate INT8 matvec: digit planes and exponents of G per direction
+  // (0: rows, 1: columns), and the per-launch digit image of the vector block
+  DevMem m_oz_a[2], m_oz_aexp[2];
+  mutable DevMem m_oz_b, m_oz_bexp;
   // factor
   DevMem theta, theta64, lval, bad, fscratch;
   // PCG workspaces
@@ -72,6 +79,9 @@ struct Solver {
   mbc_status create(const Plan &pl, const mbc_operator &o, int32_t prec, cudaStream_t st);
   mbc_status ensure_events(int count);
   mbc_status check_device_error(cudaStream_t st);
+  // INT8 FP64 matvec selected: build the digit planes if missing and size the
+  // vector image for R columns (no-op otherwise)
+  mbc_status ensure_oz(cudaStream_t st, int R);
   mbc_status factor(cudaStream_t st);
   mbc_status solve(int R, const void *rhs, int32_t rhs_dt, void *X, int32_t x_dt, const void *X0,
                    bool adjoint, const mbc_solve_options &o, mbc_solve_stats *stats,

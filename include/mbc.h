@@ -144,6 +144,30 @@ typedef enum {
 mbc_status mbc_solver_set_matvec(mbc_solver *s, int32_t impl);
 
 typedef enum {
+  MBC_FP64_MATVEC_SIMT = 0, /* FP64 CUDA-core kernels (the default) */
+  MBC_FP64_MATVEC_INT8 = 1  /* FP64-accurate INT8 tensor-core matvec (exact digit slicing) */
+} mbc_fp64_matvec;
+
+/* Choose how the FP64 matvecs of a point-kernel solver run: the FP64 solve,
+ * the FP64 residuals and polish of the mixed solve, and mbc_apply_K /
+ * mbc_apply_KT of an FP64 solver.  The INT8 form stores G as five signed
+ * 8-bit digit planes per direction, scaled by a power of two per row and
+ * 2048-column chunk (2 x 5 x nf x n bytes of device memory), and forms the
+ * products exactly in INT32 on the tensor cores.  An output is within
+ * 2^-33 sum_chunks 2048 max|G| max|v| of the exact product (about 2e-10
+ * relative on MFS operators).  The FP64 PCG then converges only on
+ * residuals recomputed with the same operator.
+ * Requested FP64 true residuals (true_residual option) always use the FP64
+ * kernels.  The planes are built by mbc_solver_prepare or by the first call
+ * that needs them (MBC_NO_MEMORY if they do not fit).  Dense operators:
+ * MBC_UNSUPPORTED. */
+mbc_status mbc_solver_set_fp64_matvec(mbc_solver *s, int32_t impl);
+
+/* Build the operator data the selected matvec implementations need (the INT8
+ * digit planes) now, on `stream`, instead of inside the first solve. */
+mbc_status mbc_solver_prepare(mbc_solver *s, mbc_stream stream);
+
+typedef enum {
   MBC_SCHED_BATCHED = 0, /* all R columns advance together (per-column alpha, beta, stop) */
   MBC_SCHED_PER_RHS = 1  /* one cold-started PCG per column, in order (the reference's loop) */
 } mbc_schedule;

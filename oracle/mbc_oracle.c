@@ -747,6 +747,120 @@ void orc_mesh_rhs(int n_faces, const double *V, const int32_t *F, const int32_t 
   }
 }
 
+/* ---- INT8 digit-sliced FP64 matvec ----------------------------------------
+ * Restatement of the library's FP64-accurate INT8 tensor-core matvec (its own
+ * design, not a reference algorithm), so that the device result can be
+ * checked operation for operation:
+ *   out[i, r] = coef * sum_j G[i, j] V[j, r]
+ * over K cut into 2048-wide chunks; per chunk a power-of-two scale 2^a per
+ * row of G (largest finite |G|; non-finite G counts as 0) and 2^b per column
+ * of V (a column chunk holding a non-finite value gets b = 4096, an infinite
+ * weight); T = rint(v 2^-a 2^38) as five balanced base-256 digits (the bytes
+ * of (T + B) xor B, B = 0x8080808080); digit-pair levels l = p + q <= 4
+ * summed exactly; comb = Horner in base 256 over the levels; sum =
+ * fma((double)comb, 2^(a + b - 44), sum) chunk by chunk; out = coef * sum.
+ * Returns 0, or 1 if a level sum left the INT32 range (the device
+ * accumulators would have wrapped). */
+#define OZ_DIGITS 5
+#define OZ_W 38
+#define OZ_CHUNK 2048
+#define OZ_SHIFT 44
+#define OZ_NONFINITE 4096
+
+static double oz_pow2(int e)
+{
+  if (e < -1022) return 0.0;
+  if (e > 1023) return INFINITY;
+  const uint64_t b = (uint64_t)(e + 1023) << 52;
+  double d;
+  memcpy(&d, &b, sizeof d);
+  return d;
+}
+
+static int oz_ceil_exp2(double m)
+{
+  uint64_t b;
+  memcpy(&b, &m, sizeof b);
+  const int E = (int)((b >> 52) & 0x7FF);
+  if (E == 0) return b == 0 ? 0 : -1022;
+  return E - 1023 + ((b & 0xFFFFFFFFFFFFFull) != 0 ? 1 : 0);
+}
+
+static void oz_digits(double v, int a, int8_t *d)
+{
+  const long long T = llrint((v * oz_pow2(-a)) * oz_pow2(OZ_W));
+  const uint64_t tb = ((uint64_t)T + 0x8080808080ull) ^ 0x8080808080ull;
+  for (int p = 0; p < OZ_DIGITS; ++p) d[p] = (int8_t)(uint8_t)((tb >> (8 * (OZ_DIGITS - 1 - p))) & 0xFF);
+}
+
+int orc_oz_apply(int M, int K, int R, const double *G, const double *V, double coef, double *out)
+{
+  const int nch = (K + OZ_CHUNK - 1) / OZ_CHUNK;
+  double *sum = (double *)calloc((size_t)M * R + 1, sizeof(double));
+  int8_t *dg = (int8_t *)malloc((size_t)M * OZ_CHUNK * OZ_DIGITS + 1);
+  int8_t *dv = (int8_t *)malloc((size_t)R * OZ_CHUNK * OZ_DIGITS + 1);
+  int *ea = (int *)malloc(sizeof(int) * ((size_t)M + 1));
+  int *eb = (int *)malloc(sizeof(int) * ((size_t)R + 1));
+  int bad = 0;
+  for (int c = 0; c < nch; ++c) {
+    const int k0 = c * OZ_CHUNK;
+    const int kc = K - k0 < OZ_CHUNK ? K - k0 : OZ_CHUNK;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < M; ++i) {
+      double m = 0.0;
+      for (int j = 0; j < kc; ++j) {
+        const double g = G[(size_t)i * K + k0 + j];
+        if (isfinite(g)) m = fmax(m, fabs(g));
+      }
+      ea[i] = oz_ceil_exp2(m);
+      for (int j = 0; j < kc; ++j) {
+        const double g = G[(size_t)i * K + k0 + j];
+        int8_t *d = dg + ((size_t)i * OZ_CHUNK + j) * OZ_DIGITS;
+        if (isfinite(g)) oz_digits(g, ea[i], d);
+        else memset(d, 0, OZ_DIGITS);
+      }
+    }
+    for (int r = 0; r < R; ++r) {
+      double m = 0.0;
+      int finite = 1;
+      for (int j = 0; j < kc; ++j) {
+        const double v = V[(size_t)(k0 + j) * R + r];
+        finite = finite && isfinite(v);
+        m = fmax(m, fabs(v));
+      }
+      eb[r] = finite && isfinite(m) ? oz_ceil_exp2(m) : OZ_NONFINITE;
+      for (int j = 0; j < kc; ++j)
+        oz_digits(V[(size_t)(k0 + j) * R + r], eb[r], dv + ((size_t)r * OZ_CHUNK + j) * OZ_DIGITS);
+    }
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (int i = 0; i < M; ++i) {
+      for (int r = 0; r < R; ++r) {
+        long long acc[OZ_DIGITS] = {0, 0, 0, 0, 0};
+        for (int j = 0; j < kc; ++j) {
+          const int8_t *a = dg + ((size_t)i * OZ_CHUNK + j) * OZ_DIGITS;
+          const int8_t *b = dv + ((size_t)r * OZ_CHUNK + j) * OZ_DIGITS;
+          for (int p = 0; p < OZ_DIGITS; ++p)
+            for (int q = 0; p + q < OZ_DIGITS; ++q) acc[p + q] += (long long)a[p] * (long long)b[q];
+        }
+        long long comb = 0;
+        for (int l = 0; l < OZ_DIGITS; ++l) {
+          if (acc[l] > 2147483647ll || acc[l] < -2147483648ll) bad = 1;
+          comb = comb * 256 + acc[l];
+        }
+        double *s = sum + (size_t)i * R + r;
+        *s = fma((double)comb, oz_pow2(ea[i] + eb[r] - OZ_SHIFT), *s);
+      }
+    }
+  }
+  for (size_t t = 0; t < (size_t)M * R; ++t) out[t] = coef * sum[t];
+  free(sum);
+  free(dg);
+  free(dv);
+  free(ea);
+  free(eb);
+  return bad;
+}
+
 int orc_num_threads(void)
 {
 #ifdef _OPENMP

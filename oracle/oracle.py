@@ -59,6 +59,7 @@ def lib():
         L.orc_mesh_solid_angle.argtypes = [C.c_int, _f64p, _i32p, C.c_int, _f64p, _f64p]
         L.orc_mesh_solid_angle.restype = None
         L.orc_mesh_rhs.argtypes = [C.c_int, _f64p, _i32p, _i32p, C.c_int, _f64p, _f64p]
+        L.orc_oz_apply.argtypes = [C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.c_double, _f64p]
         L.orc_mesh_rhs.restype = None
         L.orc_added_mass.argtypes = [C.c_int, C.c_int, _f64p, _f64p, _f64p, C.c_int, _f64p, _f64p, C.c_int,
                                      _i32p, _f64p, C.c_double, _f64p]
@@ -305,6 +306,23 @@ def mesh_operator(V, F, face_body, body_pos, S):
     lib().orc_mesh_solid_angle(nfc, V, F, ns, S, M)
     lib().orc_mesh_rhs(nfc, V, F, fb, nb, bp, rhs)
     return M, rhs
+
+
+def oz_apply(G, V, coef=1.0):
+    """coef * G @ V through the INT8 digit-sliced FP64 matvec, computed the
+    way the library's INT8 tensor-core kernels compute it (orc_oz_apply).
+    Raises if a digit-level sum would overflow INT32."""
+    G = np.ascontiguousarray(G, np.float64)
+    V = np.asarray(V, np.float64)
+    one = V.ndim == 1
+    V = np.ascontiguousarray(V[:, None] if one else V)
+    M, K = G.shape
+    R = V.shape[1]
+    assert V.shape[0] == K
+    out = np.empty((M, R))
+    if lib().orc_oz_apply(M, K, R, G, V, float(coef), out) != 0:
+        raise OverflowError("INT8 digit-level sum outside the INT32 range")
+    return out[:, 0] if one else out
 
 
 def num_threads() -> int:
