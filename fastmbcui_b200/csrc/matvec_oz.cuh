@@ -648,6 +648,9 @@ __global__ void __launch_bounds__(kThreads, 1) oz_mma_kernel(OzArgs a)
   }
   if (tid == 0 && *s_fail && a.err) atomicExch(a.err, 1);
   if (warp == 0) {
+    // warp 0 is also the loader, whose lane 0 ran alone: reconverge before
+    // the warp-wide (.sync.aligned) dealloc
+    __syncwarp();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS) : "memory");
   }
