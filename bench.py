@@ -209,7 +209,7 @@ def run_trajectory(args):
         if args.warm == "learned":
             pairs = W.neighbour_pairs(scenes[k].centers)
             f = W.pair_features(pairs, q[k - 1], q[k], base.centers, base.meta["axes"], base.meta["rot"])
-            return ws.apply(hist[-1], U, sb, base.n_bodies, pairs, f)
+            return ws.apply(hist[-1].float(), U, sb, base.n_bodies, pairs, f).to(hist[-1].dtype)
         # polynomial extrapolation along the smooth trajectory (quadratic once
         # three steps are known): ~40 % fewer FP64 iterations than x(t-1)
         if len(hist) >= 3:
@@ -218,18 +218,26 @@ def run_trajectory(args):
             return 2.0 * hist[-1] - hist[-2]
         return hist[-1]
 
-    def step(k, hist, profile=0):
-        x, nx, y = coords[k]
-        X0 = start(k, hist)
-        s = F.Solver(plans[k], x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F32)
+    out_dt = torch.float64 if args.solver == "fp64" else torch.float32
+
+    def solve_scene(plan, x, nx, y, Fk, X0, profile=0):
+        """One step's factor and solve through the selected path."""
+        if args.solver == "fp64":
+            # FP64 PCG with the FP64 factor; with --fp64-matvec int8 its
+            # matvecs run on the INT8 tensor cores
+            s64 = F.Solver(plan, x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64)
+            s64.set_fp64_matvec(args.fp64_matvec).factor()
+            return s64.solve(Fk, X0=X0, out_dtype=torch.float64, profile=profile, tol=1e-8,
+                             max_iters=args.max_iters, check_every=8)
+        s = F.Solver(plan, x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F32)
         s.set_matvec(MATVEC[args.matvec]).set_fp64_matvec(args.fp64_matvec).factor()
         if args.solver == "flexible":
             # FP64 flexible CG around the FP32 PCG; the FP64 solver only applies K
             from fastmbcui_b200.flexible import solve_flexible
 
-            s64 = F.Solver(plans[k], x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64)
+            s64 = F.Solver(plan, x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64)
             s64.set_fp64_matvec(args.fp64_matvec)
-            X, info = solve_flexible(s64, s, Fm[k], tol=1e-8, inner_iters=args.inner_iters, X0=X0,
+            X, info = solve_flexible(s64, s, Fk, tol=1e-8, inner_iters=args.inner_iters, X0=X0,
                                      profile=bool(profile))
             st = {"iters_max": info["fp32_inner_iterations"], "iters_total": info["fp32_inner_iterations"] * R,
                   "refinements": info["fp64_applies"], "n_polished": 0, "true_relres_max": info["relres_max"],
@@ -238,8 +246,11 @@ def run_trajectory(args):
                   "t_matvec_ms": info["t_matvec64_ms"] + info["t_matvec32_ms"],
                   "n_matvec64": info["n_matvec64"], "t_matvec64_ms": info["t_matvec64_ms"]}
             return X.float(), st
-        X, st = s.solve(Fm[k], X0=X0, out_dtype=torch.float32, profile=profile, **opts)
-        return X, st
+        return s.solve(Fk, X0=X0, out_dtype=torch.float32, profile=profile, **opts)
+
+    def step(k, hist, profile=0):
+        x, nx, y = coords[k]
+        return solve_scene(plans[k], x, nx, y, Fm[k], start(k, hist), profile)
 
     hist = []
     cold = None
@@ -271,25 +282,23 @@ def run_trajectory(args):
     # steps' host strengths in, host strengths out, the host plan included
     k = nsteps
     sc = scenes[k]
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory()
+    pin = lambda a, dt=np.float32: torch.from_numpy(np.ascontiguousarray(a, dt)).pin_memory()
     hx, hnx, hy, hF = pin(sc.x), pin(sc.nx), pin(sc.y), pin(sc.rhs())
-    hH = [pin(h.cpu().numpy()) for h in hist]
-    hX = torch.empty((sc.n, R), dtype=torch.float32).pin_memory()
+    hH = [pin(h.cpu().numpy(), h.cpu().numpy().dtype) for h in hist]
+    hX = torch.empty((sc.n, R), dtype=out_dt).pin_memory()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     dx, dnx, dy, dF = (a.to(dev, non_blocking=True) for a in (hx, hnx, hy, hF))
     dH = [h.to(dev, non_blocking=True) for h in hH]
     pl2 = F.Plan(sc.y.astype(np.float64), sc.rho, sc.lam, sc.max_super)
-    s2 = F.Solver(pl2, x=dx, nx=dnx, y=dy, coef=sc.coef, precision=F.MBC_F32)
-    s2.set_matvec(MATVEC[args.matvec]).factor()
-    X2, _ = s2.solve(dF, X0=start(k, dH), out_dtype=torch.float32, **opts)
+    X2, _ = solve_scene(pl2, dx, dnx, dy, dF, start(k, dH))
     hX.copy_(X2)
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) * 1000
     e2e = world * 1000.0 / _max_over_ranks(dist, e2e_ms)
-    h2d = sum(a.numel() * 4 for a in [hx, hnx, hy, hF] + hH)
-    d2h = hX.numel() * 4
-    del s2, pl2
+    h2d = sum(a.numel() * a.element_size() for a in [hx, hnx, hy, hF] + hH)
+    d2h = hX.numel() * hX.element_size()
+    del X2, pl2
 
     # plain FP64 GPU path on the first timed step: one cold-started PCG per
     # column, a bounded sample of columns extrapolated to all R
@@ -323,8 +332,10 @@ def run_trajectory(args):
         "data": "synthetic (seeded trajectory)",
         "config": {"workload": "trajectory32", "desc": WORKLOADS["trajectory32"][1], "N": base.n,
                    "Nf": base.nf, "R": R, "rho": base.rho, "lambda": base.lam, "tol": 1e-8,
-                   "precision": ("FP64 flexible CG around FP32 PCG" if args.solver == "flexible"
-                                 else "mixed FP32/FP64 residual replacement"), "schedule": "batched",
+                   "precision": {"flexible": "FP64 flexible CG around FP32 PCG",
+                                 "fp64": "FP64 PCG, FP64 factor",
+                                 "mixed": "mixed FP32/FP64 residual replacement"}[args.solver],
+                   "schedule": "batched",
                    "warm_start": {"learned": "previous step + MLP correction (3x256, BF16 weights)",
                                   "extrapolate": "quadratic extrapolation of the last three steps' strengths",
                                   "previous": "previous step's strengths", "cold": "x0 = 0"}[args.warm],
@@ -733,8 +744,9 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=572)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scenes", type=int, default=8, help="uneven workload: scenes in the sample")
-    ap.add_argument("--solver", default="mixed", choices=["mixed", "flexible"],
-                    help="trajectory: residual-replacement mixed PCG, or FP64 flexible CG around the FP32 PCG")
+    ap.add_argument("--solver", default="mixed", choices=["mixed", "flexible", "fp64"],
+                    help="trajectory: residual-replacement mixed PCG, FP64 flexible CG around the FP32 PCG, "
+                         "or FP64 PCG (pair with --fp64-matvec int8)")
     ap.add_argument("--inner-iters", type=int, default=40, help="flexible solver: FP32 iterations per outer step")
     ap.add_argument("--plan-every", type=int, default=1,
                     help="trajectory: rebuild the host plan every K steps (K > 1 reuses it, not the plain method)")
