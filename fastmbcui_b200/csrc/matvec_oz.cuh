@@ -203,8 +203,8 @@ template <int DIR>
 __global__ void __launch_bounds__(256) oz_digits_kernel(const float4 *__restrict__ xr,
                                                         const float4 *__restrict__ nr,
                                                         const float4 *__restrict__ ys, int nf, int n,
-                                                        int8_t *__restrict__ adig,
-                                                        int32_t *__restrict__ aexp,
+                                                        int8_t *__restrict__ adig, size_t adig_size,
+                                                        int32_t *__restrict__ aexp, size_t aexp_size,
                                                         int32_t *__restrict__ err)
 {
   extern __shared__ float4 sco[];
@@ -266,19 +266,24 @@ __global__ void __launch_bounds__(256) oz_digits_kernel(const float4 *__restrict
       }
     }
   }
-  if (bad) atomicExch(err, 3);
+  if (bad) atomicMax(err, 3);
   int ea[4];
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
 #pragma unroll
     for (int o = 1; o < 8; o <<= 1) mx[u] = fmax(mx[u], __shfl_xor_sync(0xffffffffu, mx[u], o));
     ea[u] = ceil_exp2(mx[u]);
-    if (c16 == 0) aexp[aexp_index(rt, c, 32 * u + 4 * warp + sub, nchunks)] = ea[u];
+    const size_t ei = aexp_index(rt, c, 32 * u + 4 * warp + sub, nchunks);
+    if (c16 == 0) {
+      if (ei < aexp_size) aexp[ei] = ea[u];
+      else atomicMax(err, 4);
+    }
   }
   // pass 2: digits, one 16-byte group of five planes per (row, c16)
   for (int ks = ks0; ks < ks1; ++ks) {
     const int kk0 = (ks - ks0) * kKS + c16 * 16;
-    unsigned char *tile = reinterpret_cast<unsigned char *>(adig) + adig_offset(rt, ks, 0, nks);
+    const size_t tile_off = adig_offset(rt, ks, 0, nks);
+    unsigned char *tile = reinterpret_cast<unsigned char *>(adig) + tile_off;
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int row = 32 * u + 4 * warp + sub;
@@ -298,6 +303,10 @@ __global__ void __launch_bounds__(256) oz_digits_kernel(const float4 *__restrict
           w[p][e >> 2] |= (uint32_t)((tb >> (8 * (kDigits - 1 - p))) & 0xFFu) << (8 * (e & 3));
       }
       const uint32_t off = sw128_i8(row, c16);
+      if (tile_off + (size_t)(kDigits - 1) * kPlaneBytes + off + 16 > adig_size) {
+        atomicMax(err, 4);  // outside the planes: skip the stores
+        continue;
+      }
 #pragma unroll
       for (int p = 0; p < kDigits; ++p)
         *reinterpret_cast<uint4 *>(tile + (size_t)p * kPlaneBytes + off) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
@@ -311,9 +320,10 @@ __global__ void __launch_bounds__(256) oz_digits_kernel(const float4 *__restrict
 // bstage_bytes(np) + ...], rows p * np + r (plane p, column grp * np + r) of
 // the swizzled image; bexp[(grp * nchunks + c) * np + r].
 __global__ void __launch_bounds__(512) oz_pack_b_kernel(const double *__restrict__ vin, int K, int R,
-                                                        int np, int8_t *__restrict__ bimg,
-                                                        int32_t *__restrict__ bexp,
-                                                        const int32_t *__restrict__ done)
+                                                        int np, int8_t *__restrict__ bimg, size_t bimg_size,
+                                                        int32_t *__restrict__ bexp, size_t bexp_size,
+                                                        const int32_t *__restrict__ done,
+                                                        int32_t *__restrict__ err)
 {
   if (done && *done) return;
   __shared__ double s_max[16][kNpMax];
@@ -347,7 +357,9 @@ __global__ void __launch_bounds__(512) oz_pack_b_kernel(const double *__restrict
     for (int w = 0; w < 16; ++w) m = fmax(m, s_max[w][col]);
     const int e = isfinite(m) ? ceil_exp2(m) : kNonFinite;
     s_exp[col] = e;
-    bexp[bexp_index(grp, c, col, nchunks, np)] = e;
+    const size_t ei = bexp_index(grp, c, col, nchunks, np);
+    if (ei < bexp_size) bexp[ei] = e;
+    else atomicMax(err, 4);
   }
   __syncthreads();
   // pass 2: units (k-step, column, 16-byte group); lanes run over columns
@@ -371,7 +383,12 @@ __global__ void __launch_bounds__(512) oz_pack_b_kernel(const double *__restrict
       for (int p = 0; p < kDigits; ++p)
         w[p][e >> 2] |= (uint32_t)((tb >> (8 * (kDigits - 1 - p))) & 0xFFu) << (8 * (e & 3));
     }
-    unsigned char *img = reinterpret_cast<unsigned char *>(bimg) + bimg_offset(grp, ks, nks, np);
+    const size_t img_off = bimg_offset(grp, ks, nks, np);
+    unsigned char *img = reinterpret_cast<unsigned char *>(bimg) + img_off;
+    if (img_off + sw128_i8((kDigits - 1) * np + col, c16) + 16 > bimg_size) {
+      atomicMax(err, 4);  // outside the image: skip the stores
+      continue;
+    }
 #pragma unroll
     for (int p = 0; p < kDigits; ++p)
       *reinterpret_cast<uint4 *>(img + sw128_i8(p * np + col, c16)) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
@@ -425,13 +442,16 @@ struct OzArgs {
   const int32_t *aexp;  // A exponents [row tile][chunk][128]
   const int8_t *bimg;   // B image of the input block
   const int32_t *bexp;  // B exponents [group][chunk][np]
+  size_t adig_size, bimg_size;  // bytes
+  size_t aexp_size, bexp_size;  // entries
   double *out;          // M x R
   int M, K, R, groups;  // outputs, reduction length, columns, column groups
   double coef;
   const double *pdot;   // columns: p (M x R) for the curvature partials, or NULL
   double *part;         // columns: per-row-tile partials (row tiles x R)
   const int32_t *done;  // PCG all-stopped flag (may be NULL)
-  int32_t *err;         // 1: a bounded wait expired; 2: shared memory misaligned
+  int32_t *err;         // the largest code raised (atomicMax): 1 a bounded wait expired, 2 shared
+                        // memory misaligned, 4 an index outside its buffer (access skipped)
 };
 
 // NPH = np / 2 columns per accumulator warp
@@ -445,7 +465,7 @@ __global__ void __launch_bounds__(kThreads, 1) oz_mma_kernel(OzArgs a)
   static_assert(NPH % 8 == 0 && NP <= kNpMax, "columns per CTA");
   extern __shared__ __align__(1024) unsigned char smem[];
   if (tc::smem_u32(smem) & 1023u) {
-    if (threadIdx.x == 0) atomicExch(a.err, 2);
+    if (threadIdx.x == 0) atomicMax(a.err, 2);
     return;
   }
   unsigned char *aring = smem;
@@ -509,18 +529,30 @@ __global__ void __launch_bounds__(kThreads, 1) oz_mma_kernel(OzArgs a)
           *s_fail = 1;
           break;
         }
+        const size_t boff = bimg_offset(grp, ks, nks, NP);
+        if (boff + BST > a.bimg_size) {
+          atomicMax(a.err, 4);  // outside the image: no copy, fail
+          *s_fail = 1;
+          break;
+        }
         tc::mbar_arrive_tx(&bfull[sb], BST);
-        tc::bulk_g2s(bring + sb * BST, bbase + bimg_offset(grp, ks, nks, NP), BST, &bfull[sb]);
+        tc::bulk_g2s(bring + sb * BST, bbase + boff, BST, &bfull[sb]);
         ++b_issued;
         bool ok = true;
         for (int p = 0; p < kDigits; ++p) {
           const int t = ks * kDigits + p, sa = t % kASlots;
+          const size_t aoff = adig_offset(rt, ks, p, nks);
+          if (aoff + kPlaneBytes > a.adig_size) {
+            atomicMax(a.err, 4);  // outside the planes: no copy, fail
+            ok = false;
+            break;
+          }
           if (!tc::mbar_wait_one(&aempty[sa], ((t / kASlots) & 1) ^ 1, 32)) {
             ok = false;
             break;
           }
           tc::mbar_arrive_tx(&afull[sa], kPlaneBytes);
-          tc::bulk_g2s(aring + sa * kPlaneBytes, abase + adig_offset(rt, ks, p, nks), kPlaneBytes, &afull[sa]);
+          tc::bulk_g2s(aring + sa * kPlaneBytes, abase + aoff, kPlaneBytes, &afull[sa]);
           ++a_issued;
         }
         if (!ok) {
@@ -601,6 +633,15 @@ __global__ void __launch_bounds__(kThreads, 1) oz_mma_kernel(OzArgs a)
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      // the check covers the whole CTA's exponents, so every accumulator
+      // thread takes the same branch (a partial exit would strand the others
+      // at the named barrier)
+      if (aexp_index(rt, c, kM - 1, nchunks) >= a.aexp_size ||
+          bexp_index(grp, c, 0, nchunks, NP) + NP > a.bexp_size) {
+        if (aw == 0 && lane == 0) atomicMax(a.err, 4);  // no fold, fail (the MMA warp's wait expires)
+        ok = false;
+        break;
+      }
       const int ea = a.aexp[aexp_index(rt, c, row, nchunks)];
       const int32_t *eb = a.bexp + bexp_index(grp, c, c0, nchunks, NP);
 #pragma unroll
@@ -646,7 +687,7 @@ __global__ void __launch_bounds__(kThreads, 1) oz_mma_kernel(OzArgs a)
     a.part[(size_t)rt * a.R + grp * NP + tid] =
         *s_fail ? 0.0 : s_red[tid] + s_red[NP + tid] + s_red[2 * NP + tid] + s_red[3 * NP + tid];
   }
-  if (tid == 0 && *s_fail && a.err) atomicExch(a.err, 1);
+  if (tid == 0 && *s_fail && a.err) atomicMax(a.err, 1);
   if (warp == 0) {
     // warp 0 is also the loader, whose lane 0 ran alone: reconverge before
     // the warp-wide (.sync.aligned) dealloc

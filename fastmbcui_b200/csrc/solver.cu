@@ -247,12 +247,17 @@ static int oz_launch(const Solver &S, int R, const double *vin, double *out, con
     return 0;
   }
   oz::oz_pack_b_kernel<<<dim3(oz::nchunks_for(K), groups), 512, 0, st>>>(
-      vin, K, R, np, (int8_t *)S.m_oz_b.ptr, (int32_t *)S.m_oz_bexp.ptr, done);
+      vin, K, R, np, (int8_t *)S.m_oz_b.ptr, S.m_oz_b.bytes, (int32_t *)S.m_oz_bexp.ptr,
+      S.m_oz_bexp.bytes / sizeof(int32_t), done, (int32_t *)S.m_err.ptr);
   oz::OzArgs a{};
   a.adig = (const int8_t *)S.m_oz_a[DIR].ptr;
   a.aexp = (const int32_t *)S.m_oz_aexp[DIR].ptr;
   a.bimg = (const int8_t *)S.m_oz_b.ptr;
   a.bexp = (const int32_t *)S.m_oz_bexp.ptr;
+  a.adig_size = S.m_oz_a[DIR].bytes;
+  a.bimg_size = S.m_oz_b.bytes;
+  a.aexp_size = S.m_oz_aexp[DIR].bytes / sizeof(int32_t);
+  a.bexp_size = S.m_oz_bexp.bytes / sizeof(int32_t);
   a.out = out;
   a.M = M;
   a.K = K;
@@ -1323,6 +1328,7 @@ mbc_status mbc::Solver::check_device_error(cudaStream_t st)
     MBC_CK(cudaMemsetAsync(m_err.ptr, 0, sizeof(int32_t), st));
     if (e == 2) return fail(MBC_CUDA_ERROR, "tensor-core matvec: shared memory window not 1024-byte aligned");
     if (e == 3) return fail(MBC_BAD_ARG, "non-finite kernel value: a source coincides with a collocation point");
+    if (e == 4) return fail(MBC_CUDA_ERROR, "INT8 matvec: an index fell outside its buffer (the access was skipped)");
     return fail(MBC_TIMEOUT, "a bounded device wait expired in the tensor-core matvec");
   }
   return MBC_OK;
@@ -1354,9 +1360,11 @@ mbc_status mbc::Solver::ensure_oz(cudaStream_t st, int R)
     MBC_TRY(oz_allow<40>());
     MBC_TRY(oz_allow<48>());
     oz::oz_digits_kernel<0><<<dim3(oz::nchunks_for(n), oz::row_tiles(nf)), 256, sm0, st>>>(
-        x4(), n4(), y4(), nf, n, (int8_t *)m_oz_a[0].ptr, (int32_t *)m_oz_aexp[0].ptr, (int32_t *)m_err.ptr);
+        x4(), n4(), y4(), nf, n, (int8_t *)m_oz_a[0].ptr, m_oz_a[0].bytes, (int32_t *)m_oz_aexp[0].ptr,
+        m_oz_aexp[0].bytes / sizeof(int32_t), (int32_t *)m_err.ptr);
     oz::oz_digits_kernel<1><<<dim3(oz::nchunks_for(nf), oz::row_tiles(n)), 256, sm1, st>>>(
-        x4(), n4(), y4(), nf, n, (int8_t *)m_oz_a[1].ptr, (int32_t *)m_oz_aexp[1].ptr, (int32_t *)m_err.ptr);
+        x4(), n4(), y4(), nf, n, (int8_t *)m_oz_a[1].ptr, m_oz_a[1].bytes, (int32_t *)m_oz_aexp[1].ptr,
+        m_oz_aexp[1].bytes / sizeof(int32_t), (int32_t *)m_err.ptr);
     launches += 2;
     MBC_CKL();
     MBC_TRY(check_device_error(st));
