@@ -192,8 +192,18 @@ __device__ __forceinline__ uint64_t digit_bytes(double v, int a)
 }
 
 // ---------------------------------------------------------------------------
-// A digit planes of G for one direction.  Grid (chunks, row tiles), 256
-// threads.  Layout: adig[((rt * nks + ks) * kDigits + p) * kPlaneBytes + ...]
+// Digit-kernel modes: exponents (pass 1: the row maxima, written to aexp),
+// digits (pass 2: the planes, with the exponents of pass 1 or, alone, read
+// back from aexp), or both.  When the planes of every row do not fit in
+// device memory, the exponents are computed once and the planes are rebuilt
+// slab by slab (rows [rt0, rt0 + gridDim.y) tiles) for every matvec.
+constexpr int kModeExps = 1;
+constexpr int kModeDigits = 2;
+
+// ---------------------------------------------------------------------------
+// A digit planes of G for one direction.  Grid (chunks, row tiles of the
+// slab), 256 threads; global row tile = rt0 + blockIdx.y, plane tile index =
+// blockIdx.y (the slab's own buffer).  Layout: adig[((rt * nks + ks) * kDigits + p) * kPlaneBytes + ...]
 // with the swizzled tile image; aexp[(rt * nchunks + c) * kM + row].  Rows or
 // K positions past the ends get digit 0.  A non-finite G (coincident point
 // and source) sets *err = 3 and counts as 0.
@@ -205,12 +215,12 @@ __global__ void __launch_bounds__(256) oz_digits_kernel(const float4 *__restrict
                                                         const float4 *__restrict__ ys, int nf, int n,
                                                         int8_t *__restrict__ adig, size_t adig_size,
                                                         int32_t *__restrict__ aexp, size_t aexp_size,
-                                                        int32_t *__restrict__ err)
+                                                        int rt0, int mode, int32_t *__restrict__ err)
 {
   extern __shared__ float4 sco[];
   const int M = DIR == 0 ? nf : n;
   const int K = DIR == 0 ? n : nf;
-  const int c = blockIdx.x, rt = blockIdx.y;
+  const int c = blockIdx.x, rt = rt0 + (int)blockIdx.y, rt_local = (int)blockIdx.y;
   const int nks = nks_for(K);
   const int nchunks = nchunks_for(K);
   const int ks0 = c * kChunkSteps;
@@ -252,7 +262,7 @@ __global__ void __launch_bounds__(256) oz_digits_kernel(const float4 *__restrict
   // pass 1: the largest |G| of each row over the chunk
   double mx[4] = {0.0, 0.0, 0.0, 0.0};
   bool bad = false;
-  for (int ks = ks0; ks < ks1; ++ks) {
+  for (int ks = ks0; ks < ((mode & kModeExps) ? ks1 : ks0); ++ks) {
     const int kk0 = (ks - ks0) * kKS + c16 * 16;
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -270,19 +280,26 @@ __global__ void __launch_bounds__(256) oz_digits_kernel(const float4 *__restrict
   int ea[4];
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
-#pragma unroll
-    for (int o = 1; o < 8; o <<= 1) mx[u] = fmax(mx[u], __shfl_xor_sync(0xffffffffu, mx[u], o));
-    ea[u] = ceil_exp2(mx[u]);
     const size_t ei = aexp_index(rt, c, 32 * u + 4 * warp + sub, nchunks);
-    if (c16 == 0) {
-      if (ei < aexp_size) aexp[ei] = ea[u];
+    if (mode & kModeExps) {
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) mx[u] = fmax(mx[u], __shfl_xor_sync(0xffffffffu, mx[u], o));
+      ea[u] = ceil_exp2(mx[u]);
+      if (c16 == 0) {
+        if (ei < aexp_size) aexp[ei] = ea[u];
+        else atomicMax(err, 4);
+      }
+    } else {
+      ea[u] = 0;
+      if (ei < aexp_size) ea[u] = aexp[ei];
       else atomicMax(err, 4);
     }
   }
+  if (!(mode & kModeDigits)) return;
   // pass 2: digits, one 16-byte group of five planes per (row, c16)
   for (int ks = ks0; ks < ks1; ++ks) {
     const int kk0 = (ks - ks0) * kKS + c16 * 16;
-    const size_t tile_off = adig_offset(rt, ks, 0, nks);
+    const size_t tile_off = adig_offset(rt_local, ks, 0, nks);
     unsigned char *tile = reinterpret_cast<unsigned char *>(adig) + tile_off;
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -444,6 +461,7 @@ struct OzArgs {
   const int32_t *bexp;  // B exponents [group][chunk][np]
   size_t adig_size, bimg_size;  // bytes
   size_t aexp_size, bexp_size;  // entries
+  int rt0;              // first row tile of this launch (slab); adig holds the slab's planes
   double *out;          // M x R
   int M, K, R, groups;  // outputs, reduction length, columns, column groups
   double coef;
@@ -484,7 +502,8 @@ __global__ void __launch_bounds__(kThreads, 1) oz_mma_kernel(OzArgs a)
   double *s_red = reinterpret_cast<double *>(tail + 256);  // [4][NP]
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int rt = blockIdx.x / a.groups, grp = blockIdx.x - rt * a.groups;
+  const int rt_local = blockIdx.x / a.groups, grp = blockIdx.x - rt_local * a.groups;
+  const int rt = a.rt0 + rt_local;  // global row tile: exponents, outputs, partials
   const int m0 = rt * kM;
   const int nks = nks_for(a.K);
   const int nchunks = nchunks_for(a.K);
@@ -541,7 +560,7 @@ __global__ void __launch_bounds__(kThreads, 1) oz_mma_kernel(OzArgs a)
         bool ok = true;
         for (int p = 0; p < kDigits; ++p) {
           const int t = ks * kDigits + p, sa = t % kASlots;
-          const size_t aoff = adig_offset(rt, ks, p, nks);
+          const size_t aoff = adig_offset(rt_local, ks, p, nks);
           if (aoff + kPlaneBytes > a.adig_size) {
             atomicMax(a.err, 4);  // outside the planes: no copy, fail
             ok = false;

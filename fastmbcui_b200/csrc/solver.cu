@@ -250,11 +250,12 @@ static int oz_launch(const Solver &S, int R, const double *vin, double *out, con
       vin, K, R, np, (int8_t *)S.m_oz_b.ptr, S.m_oz_b.bytes, (int32_t *)S.m_oz_bexp.ptr,
       S.m_oz_bexp.bytes / sizeof(int32_t), done, (int32_t *)S.m_err.ptr);
   oz::OzArgs a{};
-  a.adig = (const int8_t *)S.m_oz_a[DIR].ptr;
+  const DevMem &planes = S.oz_slab ? S.m_oz_a[0] : S.m_oz_a[DIR];
+  a.adig = (const int8_t *)planes.ptr;
   a.aexp = (const int32_t *)S.m_oz_aexp[DIR].ptr;
   a.bimg = (const int8_t *)S.m_oz_b.ptr;
   a.bexp = (const int32_t *)S.m_oz_bexp.ptr;
-  a.adig_size = S.m_oz_a[DIR].bytes;
+  a.adig_size = planes.bytes;
   a.bimg_size = S.m_oz_b.bytes;
   a.aexp_size = S.m_oz_aexp[DIR].bytes / sizeof(int32_t);
   a.bexp_size = S.m_oz_bexp.bytes / sizeof(int32_t);
@@ -268,17 +269,38 @@ static int oz_launch(const Solver &S, int R, const double *vin, double *out, con
   a.part = part;
   a.done = done;
   a.err = (int32_t *)S.m_err.ptr;
-  const unsigned grid = (unsigned)oz::row_tiles(M) * (unsigned)groups;
-  switch (np) {
-    case 16: oz_mma_launch<8>(a, grid, st); break;
-    case 32: oz_mma_launch<16>(a, grid, st); break;
-    case 48: oz_mma_launch<24>(a, grid, st); break;
-    case 64: oz_mma_launch<32>(a, grid, st); break;
-    case 80: oz_mma_launch<40>(a, grid, st); break;
-    default: oz_mma_launch<48>(a, grid, st); break;
+  auto mma = [&](int rt0, int tiles) {
+    a.rt0 = rt0;
+    const unsigned grid = (unsigned)tiles * (unsigned)groups;
+    switch (np) {
+      case 16: oz_mma_launch<8>(a, grid, st); break;
+      case 32: oz_mma_launch<16>(a, grid, st); break;
+      case 48: oz_mma_launch<24>(a, grid, st); break;
+      case 64: oz_mma_launch<32>(a, grid, st); break;
+      case 80: oz_mma_launch<40>(a, grid, st); break;
+      default: oz_mma_launch<48>(a, grid, st); break;
+    }
+  };
+  const int tiles = oz::row_tiles(M);
+  if (!S.oz_slab) {
+    mma(0, tiles);
+    S.launches += 2;
+  } else {
+    // the planes of each slab of rows, then its products
+    const int per = S.oz_slab_tiles[DIR];
+    const size_t smem = (DIR == 0 ? 1 : 2) * sizeof(float4) * oz::kChunk;
+    for (int r0 = 0; r0 < tiles; r0 += per) {
+      const int cnt = std::min(per, tiles - r0);
+      oz::oz_digits_kernel<DIR><<<dim3(oz::nchunks_for(K), cnt), 256, smem, st>>>(
+          S.x4(), S.n4(), S.y4(), S.nf, S.n, (int8_t *)planes.ptr, planes.bytes,
+          (int32_t *)S.m_oz_aexp[DIR].ptr, S.m_oz_aexp[DIR].bytes / sizeof(int32_t), r0, oz::kModeDigits,
+          (int32_t *)S.m_err.ptr);
+      mma(r0, cnt);
+      S.launches += 2;
+    }
+    ++S.launches;
   }
-  S.launches += 2;
-  return oz::row_tiles(M);
+  return tiles;
 }
 
 #define MBC_SHAPES(T, X)                                                   \
@@ -1343,11 +1365,6 @@ mbc_status mbc::Solver::ensure_oz(cudaStream_t st, int R)
     const size_t a0 = oz::adig_bytes(nf, n), a1 = oz::adig_bytes(n, nf);
     size_t free_b = 0, total_b = 0;
     MBC_CK(cudaMemGetInfo(&free_b, &total_b));
-    if (a0 + a1 + ((size_t)1 << 30) > free_b)
-      return fail(MBC_NO_MEMORY, "INT8 matvec digit planes need " + std::to_string((a0 + a1) >> 20) + " MiB, " +
-                                     std::to_string(free_b >> 20) + " MiB free");
-    MBC_TRY(m_oz_a[0].reserve(a0));
-    MBC_TRY(m_oz_a[1].reserve(a1));
     MBC_TRY(m_oz_aexp[0].reserve(sizeof(int32_t) * oz::aexp_count(nf, n)));
     MBC_TRY(m_oz_aexp[1].reserve(sizeof(int32_t) * oz::aexp_count(n, nf)));
     const size_t sm0 = sizeof(float4) * oz::kChunk, sm1 = 2 * sizeof(float4) * oz::kChunk;
@@ -1359,12 +1376,35 @@ mbc_status mbc::Solver::ensure_oz(cudaStream_t st, int R)
     MBC_TRY(oz_allow<32>());
     MBC_TRY(oz_allow<40>());
     MBC_TRY(oz_allow<48>());
+    int mode = oz::kModeExps | oz::kModeDigits;
+    oz_slab = a0 + a1 + ((size_t)1 << 30) > free_b;
+    if (!oz_slab) {
+      MBC_TRY(m_oz_a[0].reserve(a0));
+      MBC_TRY(m_oz_a[1].reserve(a1));
+    } else {
+      // the planes do not all fit: keep the exponents, and one buffer that
+      // holds the planes of a slab of rows, rebuilt for every matvec; leave
+      // room for the PCG workspaces (4 GiB or a tenth of the device)
+      const size_t keep = std::max((size_t)4 << 30, total_b / 10);
+      const size_t budget = std::min<size_t>(free_b > keep ? free_b - keep : 0, (size_t)40 << 30);
+      const size_t t0 = (size_t)oz::nks_for(n) * oz::kDigits * oz::kPlaneBytes;   // per rows tile
+      const size_t t1 = (size_t)oz::nks_for(nf) * oz::kDigits * oz::kPlaneBytes;  // per columns tile
+      if (budget < std::max(t0, t1))
+        return fail(MBC_NO_MEMORY, "INT8 matvec: not even one row tile of digit planes fits (" +
+                                       std::to_string(std::max(t0, t1) >> 20) + " MiB)");
+      oz_slab_tiles[0] = (int)std::min<size_t>(oz::row_tiles(nf), budget / t0);
+      oz_slab_tiles[1] = (int)std::min<size_t>(oz::row_tiles(n), budget / t1);
+      m_oz_a[1].release();
+      MBC_TRY(m_oz_a[0].reserve(std::max(oz_slab_tiles[0] * t0, oz_slab_tiles[1] * t1)));
+      mode = oz::kModeExps;  // exponents of every row now; planes per matvec
+    }
+    DevMem &p0 = m_oz_a[0], &p1 = oz_slab ? m_oz_a[0] : m_oz_a[1];
     oz::oz_digits_kernel<0><<<dim3(oz::nchunks_for(n), oz::row_tiles(nf)), 256, sm0, st>>>(
-        x4(), n4(), y4(), nf, n, (int8_t *)m_oz_a[0].ptr, m_oz_a[0].bytes, (int32_t *)m_oz_aexp[0].ptr,
-        m_oz_aexp[0].bytes / sizeof(int32_t), (int32_t *)m_err.ptr);
+        x4(), n4(), y4(), nf, n, (int8_t *)p0.ptr, p0.bytes, (int32_t *)m_oz_aexp[0].ptr,
+        m_oz_aexp[0].bytes / sizeof(int32_t), 0, mode, (int32_t *)m_err.ptr);
     oz::oz_digits_kernel<1><<<dim3(oz::nchunks_for(nf), oz::row_tiles(n)), 256, sm1, st>>>(
-        x4(), n4(), y4(), nf, n, (int8_t *)m_oz_a[1].ptr, m_oz_a[1].bytes, (int32_t *)m_oz_aexp[1].ptr,
-        m_oz_aexp[1].bytes / sizeof(int32_t), (int32_t *)m_err.ptr);
+        x4(), n4(), y4(), nf, n, (int8_t *)p1.ptr, p1.bytes, (int32_t *)m_oz_aexp[1].ptr,
+        m_oz_aexp[1].bytes / sizeof(int32_t), 0, mode, (int32_t *)m_err.ptr);
     launches += 2;
     MBC_CKL();
     MBC_TRY(check_device_error(st));

@@ -37,6 +37,8 @@ struct Solver {
   int32_t fp64_matvec = MBC_FP64_MATVEC_SIMT;
   bool oz_ready = false;  // INT8 digit planes of G built for the current geometry
   mutable bool oz_unprepared = false;  // an INT8 launch found its buffers unsized (not run)
+  bool oz_slab = false;   // planes rebuilt per matvec, slab by slab (they do not all fit)
+  int oz_slab_tiles[2] = {0, 0};  // row tiles per slab, per direction
   std::vector<cudaEvent_t> events;
   std::vector<float> prof_ms_all;
   std::vector<int> prof_is64;  // 1: the pair ran in FP64

@@ -59,16 +59,22 @@ class Scene:
     def n_bodies(self) -> int:
         return int(self.centers.shape[0])
 
+    def moving_bodies(self) -> np.ndarray:
+        """Bodies that get rigid-mode columns (all but meta["static"])."""
+        static = set(int(b) for b in self.meta.get("static", ()))
+        return np.array([b for b in range(self.n_bodies) if b not in static], dtype=np.int64)
+
     def rhs(self) -> np.ndarray:
-        """Rigid-mode normal velocities, nf x 6*bodies (float32-exact)."""
-        nb = self.n_bodies
-        f = np.zeros((self.nf, 6 * nb), dtype=np.float64)
-        for b in range(nb):
+        """Rigid-mode normal velocities, nf x 6*(moving bodies), float32-exact;
+        the rows of static bodies (a fixed floor) are zero in every column."""
+        mv = self.moving_bodies()
+        f = np.zeros((self.nf, 6 * len(mv)), dtype=np.float64)
+        for k, b in enumerate(mv):
             rows = np.nonzero(self.row_body == b)[0]
             n = self.nx[rows]
             r = self.x[rows] - self.centers[b]
-            f[rows, 6 * b:6 * b + 3] = n
-            f[rows, 6 * b + 3:6 * b + 6] = np.cross(r, n)
+            f[rows, 6 * k:6 * k + 3] = n
+            f[rows, 6 * k + 3:6 * k + 6] = np.cross(r, n)
         return _f32(f)
 
     def body_ptr(self) -> np.ndarray:
@@ -299,6 +305,51 @@ def ellipsoids_scene(n_bodies: int, pts, seed: int, box: float = 10.0,
         parts.append((p + centers[b], n, p - offset * n + centers[b], centers[b]))
     return _assemble(f"ellipsoids{n_bodies}", parts, rho=3.0, lam=1.5, tol=1e-8,
                      meta={"axes": axes, "areas": [ellipsoid_area(ax) for ax in axes]})
+
+
+def large_scene(seed: int = 5, n_boxes: int = 20, box_pts: int = 5000, floor=(400, 250),
+                spacing: float = 0.05, side_range=(0.3, 1.0)) -> Scene:
+    """The large configuration: ``n_boxes`` boxes (edge U[0.3, 1], ``box_pts``
+    area-uniform points each, random orientation) above a flat floor patch of
+    400 x 250 collocation points on a square grid of ``spacing`` (normal +z).
+    N = Nf = 200000 at the defaults, rho = 4, supernodes up to 512 wide.
+
+    Sources sit 0.6 point spacings inside each box along the face normal and
+    0.6 spacings below the floor (the ratio of the ellipsoid scenes, 0.05 /
+    0.08).  Boxes do not touch one another (bounding spheres 0.1 apart) and
+    clear the floor by 0.1.  The floor is static: rhs() has rigid-mode
+    columns for the boxes only (R = 120 at the defaults).  Body n_boxes is
+    the floor; its "center" is the patch centre."""
+    rng = np.random.default_rng(seed)
+    nxg, nyg = floor
+    Lx, Ly = (nxg - 1) * spacing, (nyg - 1) * spacing
+    sides = rng.uniform(side_range[0], side_range[1], n_boxes)
+    radii = sides * np.sqrt(3.0) / 2.0
+    centers = []
+    for b in range(n_boxes):
+        for _ in range(100000):
+            c = np.array([rng.uniform(radii[b] + 0.5, Lx - radii[b] - 0.5),
+                          rng.uniform(radii[b] + 0.5, Ly - radii[b] - 0.5),
+                          rng.uniform(radii[b] + 0.1, radii[b] + 2.5)])
+            if all(np.linalg.norm(c - centers[k]) > radii[b] + radii[k] + 0.1 for k in range(len(centers))):
+                centers.append(c)
+                break
+        else:
+            raise RuntimeError("could not place the boxes")
+    parts = []
+    for b in range(n_boxes):
+        p, n = sample_box(rng, box_pts, sides[b])
+        h = np.sqrt(6.0 * sides[b] ** 2 / box_pts)
+        R = random_rotation(rng)
+        p, n = p @ R.T, n @ R.T
+        parts.append((p + centers[b], n, p - 0.6 * h * n + centers[b], centers[b]))
+    gx, gy = np.meshgrid(np.arange(nxg) * spacing, np.arange(nyg) * spacing, indexing="ij")
+    fp = np.stack([gx.ravel(), gy.ravel(), np.zeros(gx.size)], 1)
+    fn = np.tile([0.0, 0.0, 1.0], (fp.shape[0], 1))
+    parts.append((fp, fn, fp - 0.6 * spacing * fn, np.array([Lx / 2, Ly / 2, 0.0])))
+    areas = [6.0 * s_ ** 2 for s_ in sides] + [nxg * nyg * spacing ** 2]
+    return _assemble(f"large{n_boxes}", parts, rho=4.0, lam=1.5, max_super=512, tol=1e-8,
+                     meta={"sides": sides, "areas": areas, "static": [n_boxes], "spacing": spacing})
 
 
 def fibonacci_sphere(npts: int) -> np.ndarray:

@@ -29,17 +29,24 @@ static long fails = 0;
     }                                    \
   } while (0)
 
-// oz_digits_kernel<DIR> for M outputs and reduction length K
-static void check_digits(int M, int K, bool full)
+// oz_digits_kernel<DIR> for M outputs and reduction length K, over the row
+// tiles [rt0, rt0 + cnt) into a plane buffer of abytes (the whole matrix:
+// rt0 = 0, cnt = all tiles; a slab: the slab's tiles at the buffer's start)
+static void check_digits(int M, int K, bool full, int rt0 = 0, int cnt = -1, size_t abytes = 0)
 {
-  const size_t abytes = adig_bytes(M, K), ecount = aexp_count(M, K);
   const int nks = nks_for(K), nch = nchunks_for(K), nrt = row_tiles(M);
-  CHECK(nrt <= 65535, "digits: grid.y %d", nrt);
-  std::vector<unsigned char> cover(full ? abytes : 0, 0);
-  std::vector<unsigned char> ecover(full ? ecount : 0, 0);
+  if (cnt < 0) cnt = nrt;
+  if (abytes == 0) abytes = adig_bytes(M, K);
+  const size_t ecount = aexp_count(M, K);
+  CHECK(cnt <= 65535 && rt0 + cnt <= nrt, "digits: grid.y %d at %d of %d", cnt, rt0, nrt);
+  const size_t used = (size_t)cnt * nks * kDigits * kPlaneBytes;  // bytes the launch must fill
+  CHECK(used <= abytes, "digits: %zu plane bytes > buffer %zu", used, abytes);
+  std::vector<unsigned char> cover(full ? used : 0, 0);
+  std::vector<unsigned char> ecover(full && rt0 == 0 && cnt == nrt ? ecount : 0, 0);
   for (int c = 0; c < nch; ++c) {
-    for (int rt = 0; rt < nrt; ++rt) {
-      if (!full && !(rt == 0 || rt == nrt - 1) && !(c == 0 || c == nch - 1)) continue;
+    for (int rl = 0; rl < cnt; ++rl) {
+      const int rt = rt0 + rl;
+      if (!full && !(rl == 0 || rl == cnt - 1) && !(c == 0 || c == nch - 1)) continue;
       const int ks0 = c * kChunkSteps, ks1 = std::min(ks0 + kChunkSteps, nks);
       const int kbase = ks0 * kKS, kcount = std::min(kChunk, K - kbase);
       CHECK(kcount > 0 && kbase + kcount <= K, "digits: chunk %d range", c);
@@ -49,18 +56,16 @@ static void check_digits(int M, int K, bool full)
           for (int u = 0; u < 4; ++u) {
             const int row = 32 * u + 4 * warp + sub;
             CHECK(row >= 0 && row < kM, "digits: row %d", row);
-            if (c16 == 0) {
-              const size_t ei = aexp_index(rt, c, row, nch);
-              CHECK(ei < ecount, "digits: aexp index %zu >= %zu", ei, ecount);
-              if (full) ++ecover[ei];
-            }
+            const size_t ei = aexp_index(rt, c, row, nch);
+            CHECK(ei < ecount, "digits: aexp index %zu >= %zu", ei, ecount);
+            if (c16 == 0 && !ecover.empty() && ei < ecount) ++ecover[ei];
             for (int ks = ks0; ks < ks1; ++ks) {
               const int kk0 = (ks - ks0) * kKS + c16 * 16;
               CHECK(kk0 >= 0 && kk0 + 15 < kChunk, "digits: staged index %d", kk0 + 15);
               for (int p = 0; p < kDigits; ++p) {
-                const size_t off = adig_offset(rt, ks, 0, nks) + (size_t)p * kPlaneBytes + sw128_i8(row, c16);
+                const size_t off = adig_offset(rl, ks, 0, nks) + (size_t)p * kPlaneBytes + sw128_i8(row, c16);
                 CHECK(off % 16 == 0 && off + 16 <= abytes, "digits: store at %zu (+16) > %zu", off, abytes);
-                if (full && off + 16 <= abytes)
+                if (full && off + 16 <= used)
                   for (int b = 0; b < 16; ++b) ++cover[off + b];
               }
             }
@@ -69,8 +74,9 @@ static void check_digits(int M, int K, bool full)
     }
   }
   if (full) {
-    for (size_t i = 0; i < abytes; ++i) CHECK(cover[i] == 1, "digits: byte %zu written %d times", i, cover[i]);
-    for (size_t i = 0; i < ecount; ++i) CHECK(ecover[i] == 1, "digits: exponent %zu written %d times", i, ecover[i]);
+    for (size_t i = 0; i < used; ++i) CHECK(cover[i] == 1, "digits: byte %zu written %d times", i, cover[i]);
+    for (size_t i = 0; i < ecover.size(); ++i)
+      CHECK(ecover[i] == 1, "digits: exponent %zu written %d times", i, ecover[i]);
   }
 }
 
@@ -114,19 +120,23 @@ static void check_pack(int K, int R, bool full)
 }
 
 // oz_mma_kernel for M outputs, K reduction, R columns; part_rows: rows of the
-// curvature-partials buffer the columns direction writes (0: none)
-static void check_mma(int M, int K, int R, int part_rows)
+// curvature-partials buffer the columns direction writes (0: none); a slab
+// launch covers row tiles [rt0, rt0 + cnt) with the slab's planes in abytes
+static void check_mma(int M, int K, int R, int part_rows, int rt0 = 0, int cnt = -1, size_t abytes = 0)
 {
   const int np = np_for(R), groups = groups_for(R), nks = nks_for(K), nch = nchunks_for(K);
-  const int nrt = row_tiles(M), BST = bstage_bytes(np), TC = tmem_cols_for(np);
-  const size_t abytes = adig_bytes(M, K), bbytes = bimg_bytes(K, R);
+  const int nrt_all = row_tiles(M), BST = bstage_bytes(np), TC = tmem_cols_for(np);
+  const int nrt = cnt < 0 ? nrt_all : cnt;
+  if (abytes == 0) abytes = adig_bytes(M, K);
+  const size_t bbytes = bimg_bytes(K, R);
+  CHECK(rt0 + nrt <= nrt_all, "mma: slab %d + %d > %d", rt0, nrt, nrt_all);
   CHECK((long long)nrt * groups < (1ll << 31), "mma: grid %d x %d", nrt, groups);
   CHECK(smem_bytes(np) <= kSmemLimit, "mma: shared memory %d", smem_bytes(np));
   CHECK(kPlaneBytes % 1024 == 0 && BST % 1024 == 0, "mma: stage alignment");
   CHECK((2 * kASlots + 2 * kBSlots + 3) * 8 + 4 + 4 + 8 <= 256, "mma: barrier tail");
   CHECK(tail_bytes(np) >= 256 + 4 * np * 8, "mma: partials tail");
   CHECK(TC >= kLevels * np && TC <= 512 && (TC & (TC - 1)) == 0 && TC >= 32, "mma: tensor memory %d", TC);
-  CHECK(part_rows == 0 || nrt <= part_rows, "mma: partial rows %d > %d", nrt, part_rows);
+  CHECK(part_rows == 0 || nrt_all <= part_rows, "mma: partial rows %d > %d", nrt_all, part_rows);
   for (int rt = 0; rt < nrt; ++rt)
     for (int grp = 0; grp < groups; ++grp)
       for (int ks = 0; ks < nks; ++ks) {
@@ -162,7 +172,7 @@ static void check_mma(int M, int K, int R, int part_rows)
         CHECK(l * np + c0 + g * 8 + 8 <= TC, "acc: tensor-memory column %d", l * np + c0 + g * 8 + 8);
     for (int c = 0; c < nch; ++c) {
       CHECK(bexp_index(groups - 1, c, c0 + NPH - 1, nch, np) < bexp_count(K, R), "acc: bexp index");
-      CHECK(aexp_index(nrt - 1, c, kM - 1, nch) < aexp_count(M, K), "acc: aexp index");
+      CHECK(aexp_index(rt0 + nrt - 1, c, kM - 1, nch) < aexp_count(M, K), "acc: aexp index");
     }
     for (int k = 0; k < NPH; ++k) CHECK((4 - 1) * np + c0 + k < 4 * np, "acc: s_red index");
   }
@@ -185,6 +195,37 @@ int main()
       CHECK(bexp_count(n, R) <= bexp_count(K, R) && bexp_count(nf, R) <= bexp_count(K, R), "B exponent sizing");
       check_mma(nf, n, R, 0);
       check_mma(n, nf, R, (n + 63) / 64);
+    }
+  }
+  // slab mode: the planes of `per` row tiles at a time in one buffer sized
+  // for the larger direction, exponents for every row
+  for (auto &s : small) {
+    const int nf = s[0], n = s[1];
+    for (int per : {1, 2, 3}) {
+      const size_t t0 = (size_t)nks_for(n) * kDigits * kPlaneBytes, t1 = (size_t)nks_for(nf) * kDigits * kPlaneBytes;
+      const int p0 = std::min(per, row_tiles(nf)), p1 = std::min(per, row_tiles(n));
+      const size_t buf = std::max(p0 * t0, p1 * t1);
+      for (int r0 = 0; r0 < row_tiles(nf); r0 += p0) {
+        const int cnt = std::min(p0, row_tiles(nf) - r0);
+        check_digits(nf, n, true, r0, cnt, buf);
+        for (int R : {1, 96, 192}) check_mma(nf, n, R, 0, r0, cnt, buf);
+      }
+      for (int r0 = 0; r0 < row_tiles(n); r0 += p1) {
+        const int cnt = std::min(p1, row_tiles(n) - r0);
+        check_digits(n, nf, true, r0, cnt, buf);
+        for (int R : {1, 96, 192}) check_mma(n, nf, R, (n + 63) / 64, r0, cnt, buf);
+      }
+    }
+  }
+  // the large configuration in slabs of a 40 GiB buffer: extremes only
+  {
+    const int n = 200000;
+    const size_t t = (size_t)nks_for(n) * kDigits * kPlaneBytes;
+    const int per = (int)std::min<size_t>(row_tiles(n), ((size_t)40 << 30) / t);
+    for (int r0 : {0, (row_tiles(n) - 1) / per * per}) {
+      const int cnt = std::min(per, row_tiles(n) - r0);
+      check_digits(n, n, false, r0, cnt, (size_t)per * t);
+      check_mma(n, n, 120, (n + 63) / 64, r0, cnt, (size_t)per * t);
     }
   }
   // full-size shapes: extremes only

@@ -101,17 +101,23 @@ def digit_bytes(v, a):
 
 
 # --- the three kernels --------------------------------------------------------
-def digits_kernel(G):
-    """oz_digits_kernel for the matrix G (M x K, FP64, finite)."""
+def digits_kernel(G, rt0=0, cnt=None, mode=3, aexp=None, adig=None):
+    """oz_digits_kernel for the matrix G (M x K, FP64, finite) over row tiles
+    [rt0, rt0 + cnt): mode 1 exponents, 2 digits (exponents read from aexp),
+    3 both; the planes go to the launch's own buffer (slab-local tiles)."""
     M, K = G.shape
     nks, nch = nks_for(K), nchunks_for(K)
-    adig = np.zeros(row_tiles(M) * nks * KD * PLANE, np.uint8)
-    aexp = np.zeros(row_tiles(M) * nch * KM, np.int64)
+    cnt = row_tiles(M) if cnt is None else cnt
+    if adig is None:
+        adig = np.zeros(cnt * nks * KD * PLANE, np.uint8)
+    if aexp is None:
+        aexp = np.zeros(row_tiles(M) * nch * KM, np.int64)
     for c in range(nch):
         ks0, ks1 = c * CHUNK_STEPS, min(c * CHUNK_STEPS + CHUNK_STEPS, nks)
         kbase = ks0 * KKS
         kcount = min(KCHUNK, K - kbase)
-        for rt in range(row_tiles(M)):
+        for rl in range(cnt):
+            rt = rt0 + rl
             for warp in range(8):
                 for lane in range(32):
                     sub, c16 = lane >> 3, lane & 7
@@ -119,13 +125,18 @@ def digits_kernel(G):
                         row = 32 * u + 4 * warp + sub
                         gm = rt * KM + row
                         valid = gm < M
-                        mx = np.abs(G[gm, kbase:kbase + kcount]).max() if valid else 0.0
-                        ea = ceil_exp2(mx)
-                        if c16 == 0:
-                            aexp[aexp_index(rt, c, row, nch)] = ea
+                        if mode & 1:
+                            mx = np.abs(G[gm, kbase:kbase + kcount]).max() if valid else 0.0
+                            ea = ceil_exp2(mx)
+                            if c16 == 0:
+                                aexp[aexp_index(rt, c, row, nch)] = ea
+                        else:
+                            ea = int(aexp[aexp_index(rt, c, row, nch)])
+                        if not mode & 2:
+                            continue
                         for ks in range(ks0, ks1):
                             kk0 = (ks - ks0) * KKS + c16 * 16
-                            tile = adig_offset(rt, ks, 0, nks)
+                            tile = adig_offset(rl, ks, 0, nks)
                             for e in range(16):
                                 k = kk0 + e
                                 b = digit_bytes(G[gm, kbase + k], ea) if (valid and k < kcount) else [0] * KD
@@ -174,18 +185,20 @@ def read_tile(buf, base, rows):
     return buf[idx].view(np.int8).astype(np.int64)
 
 
-def mma_kernel(adig, aexp, bimg, bexp, M, K, R, coef):
+def mma_kernel(adig, aexp, bimg, bexp, M, K, R, coef, rt0=0, cnt=None, out=None):
     np_, groups, nks, nch = np_for(R), groups_for(R), nks_for(K), nchunks_for(K)
-    out = np.zeros((M, R))
-    for blk in range(row_tiles(M) * groups):
-        rt, grp = blk // groups, blk % groups
+    cnt = row_tiles(M) if cnt is None else cnt
+    out = np.zeros((M, R)) if out is None else out
+    for blk in range(cnt * groups):
+        rl, grp = blk // groups, blk % groups
+        rt = rt0 + rl
         tmem = np.zeros((KM, 512), np.int64)
         sums = np.zeros((KM, np_))
         for ks in range(nks):
             kc = ks % CHUNK_STEPS
             B = read_tile(bimg, bimg_offset(grp, ks, nks, np_), KD * np_)
             for p in range(KD):
-                A = read_tile(adig, adig_offset(rt, ks, p, nks), KM)
+                A = read_tile(adig, adig_offset(rl, ks, p, nks), KM)
                 nt = np_ * (KD - p)
                 for kk in range(KKS // 32):
                     acc = not (kc == 0 and p == 0 and kk == 0)
@@ -229,3 +242,23 @@ def test_kernel_dataflow_equals_oracle(M, K, R):
     out = mma_kernel(adig, aexp, bimg, bexp, M, K, R, coef=-0.25)
     ref = O.oz_apply(G, V, coef=-0.25)
     assert np.array_equal(out, ref)
+
+
+def test_slab_mode_equals_full_planes():
+    """Planes rebuilt per slab of one row tile (exponents computed once, as
+    when the planes do not all fit) give the full-plane result bit for bit."""
+    M, K, R = 300, 2100, 12
+    rng = np.random.default_rng(11)
+    G = rng.standard_normal((M, K)) * 10.0 ** rng.uniform(-2, 2, (M, 1))
+    V = rng.standard_normal((K, R))
+    bimg, bexp = pack_kernel(V)
+    _, aexp = digits_kernel(G, mode=1)  # exponents of every row
+    per = 1
+    slab = np.zeros(per * nks_for(K) * KD * PLANE, np.uint8)
+    out = np.zeros((M, R))
+    for r0 in range(0, row_tiles(M), per):
+        cnt = min(per, row_tiles(M) - r0)
+        slab[:] = 0xA5  # stale bytes from the previous slab must all be overwritten
+        digits_kernel(G, rt0=r0, cnt=cnt, mode=2, aexp=aexp, adig=slab)
+        mma_kernel(slab, aexp, bimg, bexp, M, K, R, -0.25, rt0=r0, cnt=cnt, out=out)
+    assert np.array_equal(out, O.oz_apply(G, V, coef=-0.25))

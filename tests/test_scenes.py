@@ -67,3 +67,33 @@ def test_neighbour_pairs_and_features():
     assert np.isfinite(f).all() and np.isfinite(g).all()
     # the self flag marks exactly the diagonal pairs
     assert np.array_equal(g[:, 5] == 1.0, p[:, 0] == p[:, 1])
+
+
+def test_large_scene_geometry():
+    """The large configuration: 20 boxes + floor, N = Nf = 200000, R = 120
+    (the floor is static), sources inside the boxes and below the floor,
+    bodies clear of one another and of the floor."""
+    sc = S.large_scene()
+    assert sc.n == sc.nf == 200000 and sc.n_bodies == 21
+    assert sc.rho == 4.0 and sc.max_super == 512
+    F = sc.rhs()
+    assert F.shape == (200000, 120)
+    floor_rows = sc.row_body == 20
+    assert floor_rows.sum() == 100000 and np.all(F[floor_rows] == 0)
+    # every box row has a nonzero translation column of its own box
+    assert np.all(np.abs(F[~floor_rows]).max(axis=1) > 0)
+    # floor sources below the patch, box sources strictly inside their box
+    assert np.all(sc.y[sc.src_body == 20, 2] < 0) and np.all(sc.x[floor_rows, 2] == 0)
+    sides = sc.meta["sides"]
+    for b in range(20):
+        pts = sc.x[sc.row_body == b] - sc.centers[b]
+        src = sc.y[sc.src_body == b] - sc.centers[b]
+        # the rotation is unknown here: compare distances to the centre
+        assert np.linalg.norm(src, axis=1).max() < np.linalg.norm(pts, axis=1).max()
+        assert np.linalg.norm(pts, axis=1).max() <= sides[b] * np.sqrt(3) / 2 + 1e-5
+        assert (sc.x[sc.row_body == b, 2]).min() > 0.05
+    c = sc.centers[:20]
+    r = sides * np.sqrt(3) / 2
+    d = np.linalg.norm(c[:, None] - c[None], axis=-1) + np.eye(20) * 1e9
+    assert (d - r[:, None] - r[None]).min() > 0.09
+    assert np.allclose(sc.meta["areas"][:20], 6 * sides ** 2)
