@@ -1379,9 +1379,16 @@ mbc_status mbc::Solver::ensure_oz(cudaStream_t st, int R)
     int mode = oz::kModeExps | oz::kModeDigits;
     oz_slab = a0 + a1 + ((size_t)1 << 30) > free_b;
     if (!oz_slab) {
-      MBC_TRY(m_oz_a[0].reserve(a0));
-      MBC_TRY(m_oz_a[1].reserve(a1));
-    } else {
+      // concurrent solvers can take the memory between the check and the
+      // allocation: fall back to slab mode rather than fail
+      if (m_oz_a[0].reserve(a0) != MBC_OK || m_oz_a[1].reserve(a1) != MBC_OK) {
+        m_oz_a[0].release();
+        m_oz_a[1].release();
+        MBC_CK(cudaMemGetInfo(&free_b, &total_b));
+        oz_slab = true;
+      }
+    }
+    if (oz_slab) {
       // the planes do not all fit: keep the exponents, and one buffer that
       // holds the planes of a slab of rows, rebuilt for every matvec; leave
       // room for the PCG workspaces (4 GiB or a tenth of the device)
