@@ -1415,11 +1415,62 @@ mbc_status mbc::Solver::ensure_oz(cudaStream_t st, int R)
     launches += 2;
     MBC_CKL();
     MBC_TRY(check_device_error(st));
-    oz_ready = true;
+    const int K = std::max(n, nf);
+    MBC_TRY(m_oz_b.reserve(oz::bimg_bytes(K, std::max(R, 1))));
+    MBC_TRY(m_oz_bexp.reserve(sizeof(int32_t) * oz::bexp_count(K, std::max(R, 1))));
+    MBC_TRY(oz_selfcheck(st));
   }
   const int K = std::max(n, nf);
   MBC_TRY(m_oz_b.reserve(oz::bimg_bytes(K, R)));
   MBC_TRY(m_oz_bexp.reserve(sizeof(int32_t) * oz::bexp_count(K, R)));
+  return MBC_OK;
+}
+
+mbc_status mbc::Solver::oz_selfcheck(cudaStream_t st)
+{
+  // a wrong plane or kernel shows as an O(1) difference; the scheme's own
+  // error is ~1e-10 relative, so 1e-8 leaves a wide margin
+  const double tol = 1e-8;
+  MBC_TRY(m_oz_chk.reserve(sizeof(double) * (3 * (size_t)n + 2 * (size_t)nf)));
+  double *v = (double *)m_oz_chk.ptr, *t8 = v + n, *t64 = t8 + n, *w8 = t64 + n, *w64 = w8 + nf;
+  std::vector<double> hv(n);
+  uint64_t x = 0x9E3779B97F4A7C15ull;  // a fixed LCG sequence in [-1, 1)
+  for (double &e : hv) {
+    x = x * 6364136223846793005ull + 1442695040888963407ull;
+    e = (double)(x >> 11) * 0x1p-53 * 2.0 - 1.0;
+  }
+  MBC_CK(cudaMemcpyAsync(v, hv.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  oz_ready = true;
+  launch_rows<double>(*this, 1, v, w8, nullptr, st);
+  launch_cols<double>(*this, 1, w8, t8, nullptr, nullptr, nullptr, st);
+  fp64_matvec = MBC_FP64_MATVEC_SIMT;
+  launch_rows<double>(*this, 1, v, w64, nullptr, st);
+  launch_cols<double>(*this, 1, w8, t64, nullptr, nullptr, nullptr, st);
+  fp64_matvec = MBC_FP64_MATVEC_INT8;
+  MBC_CKL();
+  mbc_status e = check_device_error(st);
+  if (e != MBC_OK) {
+    oz_ready = false;
+    return e;
+  }
+  std::vector<double> h((size_t)2 * n + 2 * (size_t)nf);
+  MBC_CK(cudaMemcpyAsync(h.data(), t8, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+  MBC_CK(cudaStreamSynchronize(st));
+  auto rel = [](const double *a, const double *b, size_t m) {
+    double d = 0, r = 0;
+    for (size_t i = 0; i < m; ++i) {
+      d += (a[i] - b[i]) * (a[i] - b[i]);
+      r += b[i] * b[i];
+    }
+    return r > 0 ? std::sqrt(d / r) : std::sqrt(d);
+  };
+  const double dk = rel(h.data() + 2 * (size_t)n, h.data() + 2 * (size_t)n + nf, nf);  // w8 vs w64
+  const double dkt = rel(h.data(), h.data() + n, n);                                     // t8 vs t64
+  if (!(dk <= tol) || !(dkt <= tol)) {
+    oz_ready = false;
+    return fail(MBC_CUDA_ERROR, "INT8 matvec self-check failed: relative difference to the FP64 kernels " +
+                                    std::to_string(dk) + " (K), " + std::to_string(dkt) + " (K^T)");
+  }
   return MBC_OK;
 }
 

@@ -55,6 +55,7 @@ struct Solver {
   // (0: rows, 1: columns), and the per-launch digit image of the vector block
   DevMem m_oz_a[2], m_oz_aexp[2];
   mutable DevMem m_oz_b, m_oz_bexp;
+  DevMem m_oz_chk;  // the self-check's vectors
   // factor
   DevMem theta, theta64, lval, bad, fscratch;
   // PCG workspaces
@@ -84,6 +85,8 @@ struct Solver {
   // INT8 FP64 matvec selected: build the digit planes if missing and size the
   // vector image for R columns (no-op otherwise)
   mbc_status ensure_oz(cudaStream_t st, int R);
+  // one column through K and K^T with the INT8 and with the FP64 kernels
+  mbc_status oz_selfcheck(cudaStream_t st);
   mbc_status factor(cudaStream_t st);
   mbc_status solve(int R, const void *rhs, int32_t rhs_dt, void *X, int32_t x_dt, const void *X0,
                    bool adjoint, const mbc_solve_options &o, mbc_solve_stats *stats,

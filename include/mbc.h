@@ -159,8 +159,11 @@ typedef enum {
  * residuals recomputed with the same operator.
  * Requested FP64 true residuals (true_residual option) always use the FP64
  * kernels.  The planes are built by mbc_solver_prepare or by the first call
- * that needs them (MBC_NO_MEMORY if they do not fit).  Dense operators:
- * MBC_UNSUPPORTED. */
+ * that needs them; if the planes of every row do not fit, they are rebuilt
+ * slab by slab for each matvec (MBC_NO_MEMORY if not even one slab fits).
+ * After building, one column is checked against the FP64 kernels in both
+ * directions (MBC_CUDA_ERROR if they differ by more than 1e-8 relative).
+ * Dense operators: MBC_UNSUPPORTED. */
 mbc_status mbc_solver_set_fp64_matvec(mbc_solver *s, int32_t impl);
 
 /* Build the operator data the selected matvec implementations need (the INT8
