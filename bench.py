@@ -461,11 +461,15 @@ def run_uneven(args):
     t = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
     plans = [F.Plan(sc.y, sc.rho, sc.lam, sc.max_super) for sc in scs]
     data = [(t(sc.x), t(sc.nx), t(sc.y), t(sc.rhs())) for sc in scs]
-    opts = dict(out_dtype=torch.float32, tol=1e-8, max_iters=args.max_iters, max_refine=64, inner_tol=1e-2,
+    fp64 = args.solver == "fp64"
+    opts = dict(out_dtype=torch.float64 if fp64 else torch.float32, tol=1e-8, max_iters=args.max_iters,
                 check_every=8, graph=1)
+    if not fp64:
+        opts.update(max_refine=64, inner_tol=1e-2)
 
     def step():
-        solvers = [F.Solver(pl, x=x, nx=nx, y=y, coef=sc.coef, precision=F.MBC_F32)
+        solvers = [F.Solver(pl, x=x, nx=nx, y=y, coef=sc.coef, precision=F.MBC_F64 if fp64 else F.MBC_F32)
+                   .set_fp64_matvec(args.fp64_matvec)
                    for pl, (x, nx, y, _), sc in zip(plans, data, scs)]
         return F.solve_many(solvers, [d[3] for d in data], **opts)
 
@@ -483,7 +487,8 @@ def run_uneven(args):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
            "data": "synthetic (seeded scenes)",
            "config": {"workload": "uneven", "scenes": len(scs), "N": [sc.n for sc in scs],
-                      "R": [_ncols(sc) for sc in scs], "timing": "host wall clock around the whole sample"},
+                      "R": [_ncols(sc) for sc in scs], "timing": "host wall clock around the whole sample",
+                      "solver": "FP64 PCG" if fp64 else "mixed FP32/FP64", "fp64_matvec": args.fp64_matvec},
            "solve": {"iters_max": [int(r[1]["iters_max"]) for r in res],
                      "n_converged": [int(r[1]["n_converged"]) for r in res],
                      "true_relres_max": max(r[1]["true_relres_max"] for r in res)}}
@@ -763,8 +768,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scenes", type=int, default=8, help="uneven workload: scenes in the sample")
     ap.add_argument("--solver", default="mixed", choices=["mixed", "flexible", "fp64"],
-                    help="trajectory: residual-replacement mixed PCG, FP64 flexible CG around the FP32 PCG, "
-                         "or FP64 PCG (pair with --fp64-matvec int8)")
+                    help="trajectory and uneven: residual-replacement mixed PCG, FP64 flexible CG around the "
+                         "FP32 PCG (trajectory), or FP64 PCG (pair with --fp64-matvec int8)")
     ap.add_argument("--inner-iters", type=int, default=40, help="flexible solver: FP32 iterations per outer step")
     ap.add_argument("--plan-every", type=int, default=1,
                     help="trajectory: rebuild the host plan every K steps (K > 1 reuses it, not the plain method)")
