@@ -152,6 +152,7 @@ class Solver:
         memory per matrix entry)."""
         impl = {"simt": MBC_FP64_MATVEC_SIMT, "int8": MBC_FP64_MATVEC_INT8}.get(impl, impl)
         check(load().mbc_solver_set_fp64_matvec(self._h, int(impl)), "mbc_solver_set_fp64_matvec")
+        self.fp64_matvec = int(impl)
         return self
 
     def prepare(self):

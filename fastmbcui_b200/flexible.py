@@ -98,10 +98,15 @@ def solve_flexible(s64, s32, F, tol=1e-8, inner_iters=40, keep=20, max_outer=300
     CUDA-event time of the FP64 applications and of the inner matvecs."""
     import torch
 
+    from . import MBC_FP64_MATVEC_INT8
+
     F = F if F.dim() == 2 else F[:, None]
     F64 = F.double().contiguous()
     b = F64 if adjoint else s64.apply_KT(F64)
-    acc = {"inner": 0, "launches": 2 if not adjoint else 0, "t64": 0.0, "n64": 0, "t32": 0.0, "n32": 0}
+    # kernels per FP64 direction: one CUDA-core kernel, or pack + MMA on the INT8 path
+    per_dir = 2 if getattr(s64, "fp64_matvec", 0) == MBC_FP64_MATVEC_INT8 else 1
+    acc = {"inner": 0, "launches": (per_dir + 1) if not adjoint else 0, "t64": 0.0, "n64": 0, "t32": 0.0,
+           "n32": 0}
 
     def apply64(v):
         if profile:
@@ -113,7 +118,7 @@ def solve_flexible(s64, s32, F, tol=1e-8, inner_iters=40, keep=20, max_outer=300
             e1.synchronize()
             acc["t64"] += e0.elapsed_time(e1)
         acc["n64"] += 2
-        acc["launches"] += 4  # permute, K, K^T, permute
+        acc["launches"] += 2 + 2 * per_dir  # permute, K, K^T, permute
         return out
 
     def inner(rs):
