@@ -50,6 +50,12 @@ WORKLOADS = {
 }
 
 
+def _dtype(args, fp64_only=False):
+    """The arithmetic the timed path computes in."""
+    f64 = "f64 (int8 digit slices, exact int32 sums)" if args.fp64_matvec == "int8" else "f64"
+    return f64 if fp64_only else f"f32+{f64}"
+
+
 def _ncols(sc):
     """Rigid-mode columns of a scene (six per moving body)."""
     return 6 * len(sc.moving_bodies())
@@ -341,7 +347,7 @@ def run_trajectory(args):
     out = {
         "metric": METRIC, "value": round(value, 5), "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": _dtype(args, args.solver == "fp64"),
         "data": "synthetic (seeded trajectory)",
         "config": {"workload": "trajectory32", "desc": WORKLOADS["trajectory32"][1], "N": base.n,
                    "Nf": base.nf, "R": R, "rho": base.rho, "lambda": base.lam, "tol": 1e-8,
@@ -484,7 +490,7 @@ def run_uneven(args):
     ms = (time.perf_counter() - t0) * 1000 / args.steps
     out = {"metric": "MFS scenes solved per second (uneven batch sample, rel-res 1e-8)", "value": round(1000.0 * len(scs) / ms, 4),
            "unit": "scenes/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 1),
-           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": _dtype(args, fp64),
            "data": "synthetic (seeded scenes)",
            "config": {"workload": "uneven", "scenes": len(scs), "N": [sc.n for sc in scs],
                       "R": [_ncols(sc) for sc in scs], "timing": "host wall clock around the whole sample",
@@ -590,7 +596,7 @@ def run_ours(args):
     out = {
         "metric": METRIC, "value": round(value, 5), "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": _dtype(args),
         "data": "synthetic (seeded scene)",
         "config": {"workload": args.workload, "desc": desc, "N": sc.n, "Nf": sc.nf, "R": R,
                    "rho": sc.rho, "lambda": sc.lam, "tol": 1e-8, "precision": "mixed FP32/FP64 refine",
