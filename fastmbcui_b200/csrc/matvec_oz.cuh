@@ -215,8 +215,10 @@ __global__ void __launch_bounds__(256) oz_digits_kernel(const float4 *__restrict
                                                         const float4 *__restrict__ ys, int nf, int n,
                                                         int8_t *__restrict__ adig, size_t adig_size,
                                                         int32_t *__restrict__ aexp, size_t aexp_size,
-                                                        int rt0, int mode, int32_t *__restrict__ err)
+                                                        int rt0, int mode, const int32_t *__restrict__ done,
+                                                        int32_t *__restrict__ err)
 {
+  if (done && *done) return;  // a slab rebuild after the PCG stopped
   extern __shared__ float4 sco[];
   const int M = DIR == 0 ? nf : n;
   const int K = DIR == 0 ? n : nf;

@@ -293,7 +293,7 @@ static int oz_launch(const Solver &S, int R, const double *vin, double *out, con
       const int cnt = std::min(per, tiles - r0);
       oz::oz_digits_kernel<DIR><<<dim3(oz::nchunks_for(K), cnt), 256, smem, st>>>(
           S.x4(), S.n4(), S.y4(), S.nf, S.n, (int8_t *)planes.ptr, planes.bytes,
-          (int32_t *)S.m_oz_aexp[DIR].ptr, S.m_oz_aexp[DIR].bytes / sizeof(int32_t), r0, oz::kModeDigits,
+          (int32_t *)S.m_oz_aexp[DIR].ptr, S.m_oz_aexp[DIR].bytes / sizeof(int32_t), r0, oz::kModeDigits, done,
           (int32_t *)S.m_err.ptr);
       mma(r0, cnt);
       S.launches += 2;
@@ -1408,10 +1408,10 @@ mbc_status mbc::Solver::ensure_oz(cudaStream_t st, int R)
     DevMem &p0 = m_oz_a[0], &p1 = oz_slab ? m_oz_a[0] : m_oz_a[1];
     oz::oz_digits_kernel<0><<<dim3(oz::nchunks_for(n), oz::row_tiles(nf)), 256, sm0, st>>>(
         x4(), n4(), y4(), nf, n, (int8_t *)p0.ptr, p0.bytes, (int32_t *)m_oz_aexp[0].ptr,
-        m_oz_aexp[0].bytes / sizeof(int32_t), 0, mode, (int32_t *)m_err.ptr);
+        m_oz_aexp[0].bytes / sizeof(int32_t), 0, mode, nullptr, (int32_t *)m_err.ptr);
     oz::oz_digits_kernel<1><<<dim3(oz::nchunks_for(nf), oz::row_tiles(n)), 256, sm1, st>>>(
         x4(), n4(), y4(), nf, n, (int8_t *)p1.ptr, p1.bytes, (int32_t *)m_oz_aexp[1].ptr,
-        m_oz_aexp[1].bytes / sizeof(int32_t), 0, mode, (int32_t *)m_err.ptr);
+        m_oz_aexp[1].bytes / sizeof(int32_t), 0, mode, nullptr, (int32_t *)m_err.ptr);
     launches += 2;
     MBC_CKL();
     MBC_TRY(check_device_error(st));
