@@ -140,7 +140,8 @@ typedef enum {
 } mbc_matvec_impl;
 
 /* Choose the matvec implementation of an FP32 point-kernel solver (checks,
- * A/B timing).  FP64 and dense solvers always use the CUDA-core kernels. */
+ * A/B timing).  Dense operators always use the CUDA-core kernels; FP64
+ * matvecs follow mbc_solver_set_fp64_matvec. */
 mbc_status mbc_solver_set_matvec(mbc_solver *s, int32_t impl);
 
 typedef enum {
