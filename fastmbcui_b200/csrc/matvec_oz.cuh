@@ -418,7 +418,7 @@ __global__ void __launch_bounds__(512) oz_pack_b_kernel(const double *__restrict
 // The MMA kernel.
 
 // kind::i8, S32 accumulate, A and B signed 8-bit, K-major, M = 128, N = nn
-__device__ __forceinline__ uint32_t idesc_i8(int nn)
+__host__ __device__ __forceinline__ constexpr uint32_t idesc_i8(int nn)
 {
   return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nn >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
 }

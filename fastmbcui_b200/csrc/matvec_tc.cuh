@@ -183,7 +183,7 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 
-__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr)
+__host__ __device__ __forceinline__ constexpr uint64_t desc_sw128(uint32_t saddr)
 {
   uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);  // start address
   d |= (uint64_t)1 << 16;                            // LBO (unused for swizzled K-major)
@@ -194,7 +194,7 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr)
 }
 
 // kind::tf32, FP32 accumulate, A and B K-major, M = 128, N = np
-__device__ __forceinline__ uint32_t idesc_tf32(int np)
+__host__ __device__ __forceinline__ constexpr uint32_t idesc_tf32(int np)
 {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(np >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
 }
