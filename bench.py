@@ -451,6 +451,121 @@ def _matvec_roofline(st, nf, n, R, matvec, fp64_matvec="simt"):
             "fp64_matvec": fp64, "tensor_matvec": tc}
 
 
+def run_rows(args):
+    """Rows of the path that the solve benchmarks do not time on their own,
+    each timed with CUDA events on the launching stream after warm-up calls,
+    with its algorithmic work and the CPU oracle beside it on a bounded
+    sample; one JSON line per row:
+      R11 the adjoint solve (K^T K) X = K^T F, against the forward solve;
+      R12 the op bodies' factor cache: MinvF_float_fastGrad, then
+          VpL_fast_float and MinvF again on the same inputs;
+      R13 the added-mass reduction of the solved strengths;
+      f1  the mesh collocation matrix (solid angles) and its right-hand side.
+    FP64 work is rated against the FP64 pipe's nominal 37 TFLOP/s (no
+    measured figure), stores against the measured HBM bandwidth."""
+    import torch
+
+    import fastmbcui_b200 as F
+    import fastmbcui_b200.mfs_torch as mfs
+    from fastmbcui_b200 import mesh as MS
+    from fastmbcui_b200 import scenes as S
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    O.build()
+    dev = torch.device("cuda", 0)
+    hbm, _, src = _peaks()
+    fp64_peak = 37.0
+
+    def timed(fn, reps=1, warm=1):
+        out = None
+        for _ in range(warm):
+            out = fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, out
+
+    def emit(d):
+        print(json.dumps(d), flush=True)
+
+    sc = _scene_for("ellipsoids8", 4)
+    wl = WORKLOADS["ellipsoids8"][1]
+    t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
+    plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
+    s = F.Solver(plan, x=t(sc.x), nx=t(sc.nx), y=t(sc.y), coef=sc.coef, precision=F.MBC_F64)
+    s.set_fp64_matvec(args.fp64_matvec).factor()
+    Fm = t(sc.rhs(), torch.float64)
+    R = Fm.shape[1]
+
+    # R11: the adjoint solve of the same normal equations
+    B = s.apply_KT(Fm)
+    ms_f, (X, st_f) = timed(lambda: s.solve(Fm, tol=1e-8, max_iters=args.max_iters))
+    ms_a, (Xa, st_a) = timed(lambda: s.solve_adjoint(B, tol=1e-8, max_iters=args.max_iters))
+    emit({"row": "R11 adjoint solve", "workload": wl, "ms": round(ms_a, 2), "forward_ms": round(ms_f, 2),
+          "iters_max": int(st_a["iters_max"]), "forward_iters_max": int(st_f["iters_max"]),
+          "same_solution_rel": float(torch.linalg.norm(Xa - X) / torch.linalg.norm(X)),
+          "dtype": _dtype(args, True)})
+
+    # R12: the op bodies (dense FP32 M, the reference's interface) and their cache
+    M = t(sc.dense_K())
+    F32, Vs = t(sc.rhs()), t(sc.y)
+    pL = t(np.random.default_rng(0).standard_normal((sc.n, R)))
+    ms_first, _ = timed(lambda: mfs.ops.MinvF_float_fastGrad(M, F32, Vs, sc.rho, args.max_iters, 1e-8), warm=0)
+    ms_vpl, _ = timed(lambda: mfs.ops.VpL_fast_float(M, pL, Vs, sc.rho, args.max_iters, 1e-8), warm=0)
+    ms_again, _ = timed(lambda: mfs.ops.MinvF_float_fastGrad(M, F32, Vs, sc.rho, args.max_iters, 1e-8), warm=0)
+    emit({"row": "R12 op bodies and factor cache", "workload": wl + " (dense FP32 M)",
+          "minvf_first_ms": round(ms_first, 1), "vpl_cached_ms": round(ms_vpl, 1),
+          "minvf_cached_ms": round(ms_again, 1), "dtype": "f32 (dense M) + f64 dots"})
+    del M
+
+    # R13: added mass of the FP64 strengths
+    w, bp, cen = sc.weights(), sc.body_ptr(), sc.centers
+    ms_am, Mf = timed(lambda: s.added_mass(X, w, bp, cen), reps=3, warm=2)
+    flops = float(sc.nf) * sc.n * (2 * R + 8)
+    t0 = time.perf_counter()
+    Mo = O.added_mass(sc, X.cpu().numpy(), 1.0)
+    cpu_ms = (time.perf_counter() - t0) * 1000
+    ach = flops / (ms_am * 1e-3) / 1e12
+    emit({"row": "R13 added mass", "workload": wl, "ms": round(ms_am, 3),
+          "roofline": {"bound": "fp64", "achieved": round(ach, 2), "peak": fp64_peak, "unit": "TFLOP/s",
+                       "frac": round(ach / fp64_peak, 4), "work": f"nf n (2R + 8) = {flops:.3e} flops",
+                       "peak_source": "FP64 nominal (no measured figure)"},
+          "oracle_rel_diff": float(np.linalg.norm(Mf - Mo) / np.linalg.norm(Mo)),
+          "cpu_baseline": {"ms": round(cpu_ms, 1), "cores": O.num_threads(), "kind": "port",
+                           "sample": "the same reduction in full (orc_added_mass)"}})
+
+    # f1: mesh collocation matrix of 8 icosphere-4 bodies (40960 faces x 20496 sources)
+    bodies = [(4, (1.0, 0.8, 0.6), (0.1 * b, 0.2, 0.3), (3.0 * (b % 4), 3.0 * (b // 4), 0.0), 0.1)
+              for b in range(8)]
+    ms_ = S.mesh_scene(bodies)
+    args_m = (ms_["V"], ms_["F"], ms_["S"], ms_["face_body"], ms_["body_pos"])
+    ms_mesh, (Mm, rhs) = timed(lambda: MS.assemble(*args_m), reps=3, warm=1)
+    nfc, ns = ms_["F"].shape[0], ms_["S"].shape[0]
+    flops = 60.0 * nfc * ns
+    stored = 4.0 * nfc * ns
+    sub = 4096
+    t0 = time.perf_counter()
+    O.mesh_operator(ms_["V"], ms_["F"][:sub], ms_["face_body"][:sub], ms_["body_pos"], ms_["S"])
+    cpu_ms = (time.perf_counter() - t0) * 1000 * nfc / sub
+    ach, gbs = flops / (ms_mesh * 1e-3) / 1e12, stored / (ms_mesh * 1e-3) / 1e9
+    emit({"row": "f1 mesh collocation matrix", "workload": f"8 icosphere-4 bodies: {nfc} faces x {ns} sources, FP32 out",
+          "ms": round(ms_mesh, 2),
+          "roofline": {"bound": "fp64" if ach / fp64_peak >= gbs / hbm else "hbm",
+                       "achieved_tflops": round(ach, 2), "frac_fp64": round(ach / fp64_peak, 4),
+                       "achieved_store_gbs": round(gbs, 1), "frac_hbm": round(gbs / hbm, 4),
+                       "work": "~60 FP64 flops and 4 stored bytes per entry",
+                       "peak_source": f"FP64 nominal; HBM {src} (of measured)"},
+          "cpu_baseline": {"ms": round(cpu_ms, 1), "cores": O.num_threads(), "kind": "port",
+                           "sample": f"first {sub} faces, scaled to all {nfc}"}})
+    del Mm
+
+
 def run_uneven(args):
     """A bounded sample of the uneven batch (scenes of 1-8 ellipsoids,
     1500-8000 points per body, seeds 3...): every scene planned on the host,
@@ -791,10 +906,15 @@ def main():
                     help="with --kernel-probe: one full mixed solve instead of K / K^T launches")
     ap.add_argument("--matvec", default="auto", choices=sorted(MATVEC),
                     help="FP32 matvec: tensor cores (3xTF32 tcgen05) or CUDA cores")
+    ap.add_argument("--rows-probe", action="store_true",
+                    help="time the adjoint solve, the op bodies' cache, the added mass and the mesh assembly "
+                         "(one JSON line each)")
     ap.add_argument("--fp64-matvec", default="simt", choices=["simt", "int8"],
                     help="FP64 matvec: CUDA-core FP64 kernels or exact INT8 digit slicing on the tensor cores")
     args = ap.parse_args()
-    if args.kernel_probe:
+    if args.rows_probe:
+        run_rows(args)
+    elif args.kernel_probe:
         run_probe(args)
     elif args.impl == "reference":
         run_reference(args)
