@@ -822,6 +822,7 @@ def run_probe(args):
     V = t(rng.standard_normal((sc.n, R)))
     if f64:
         V = V.double()
+        solver.prepare()  # INT8 digit planes and their self-check, outside the timed launches
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     out = []
     for _ in range(args.probe_reps):
@@ -832,10 +833,19 @@ def run_probe(args):
         ev[2].record()
         torch.cuda.synchronize()
         out.append((ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])))
-    print(json.dumps({"probe": args.workload, "matvec": "simt" if f64 else args.matvec,
-                      "precision": args.probe_precision, "R": R,
-                      "K_ms": [round(a, 3) for a, _ in out],
-                      "KT_ms": [round(b, 3) for _, b in out]}), flush=True)
+    line = {"probe": args.workload, "matvec": args.fp64_matvec if f64 else args.matvec,
+            "precision": args.probe_precision, "R": R,
+            "K_ms": [round(a, 3) for a, _ in out],
+            "KT_ms": [round(b, 3) for _, b in out]}
+    if f64 and args.fp64_matvec == "int8":
+        # per direction: 15 digit-plane products (2 ops per MAC) and 5 plane bytes per entry
+        hbm, bf16, _ = _peaks()
+        best = min(min(a, b) for a, b in out) * 1e-3
+        line["int8"] = {"tops": round(2.0 * 15 * sc.nf * sc.n * R / best / 1e12, 1),
+                        "frac_of_int8": round(2.0 * 15 * sc.nf * sc.n * R / best / 1e12 / (2 * bf16), 4),
+                        "plane_gbs": round(5.0 * sc.nf * sc.n / best / 1e9, 1),
+                        "frac_of_hbm": round(5.0 * sc.nf * sc.n / best / 1e9 / hbm, 4)}
+    print(json.dumps(line), flush=True)
 
 
 def run_reference(args):
