@@ -247,7 +247,7 @@ def run_trajectory(args):
             s64 = F.Solver(plan, x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64)
             s64.set_fp64_matvec(args.fp64_matvec).factor()
             return s64.solve(Fk, X0=X0, out_dtype=torch.float64, profile=profile, tol=1e-8,
-                             max_iters=args.max_iters, check_every=8)
+                             max_iters=args.max_iters, check_every=8, compact=int(args.compact))
         s = F.Solver(plan, x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F32)
         s.set_matvec(MATVEC[args.matvec]).set_fp64_matvec(args.fp64_matvec).factor()
         if args.solver == "flexible":
@@ -360,6 +360,7 @@ def run_trajectory(args):
                                   "previous": "previous step's strengths", "cold": "x0 = 0"}[args.warm],
                    "steps_run": f"{args.warmup} warm-up + {args.steps} timed",
                    "plan_every": args.plan_every, "solver": args.solver, "fp64_matvec": args.fp64_matvec,
+                   "compact": bool(args.compact and args.solver == "fp64"),
                    "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas{world}"},
         "e2e": {"value": round(e2e, 5), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h),
@@ -587,6 +588,8 @@ def run_uneven(args):
                 check_every=8, graph=1)
     if not fp64:
         opts.update(max_refine=64, inner_tol=1e-2)
+    else:
+        opts.update(compact=int(args.compact))
 
     def step():
         solvers = [F.Solver(pl, x=x, nx=nx, y=y, coef=sc.coef, precision=F.MBC_F64 if fp64 else F.MBC_F32)
@@ -916,6 +919,8 @@ def main():
                     help="with --kernel-probe: one full mixed solve instead of K / K^T launches")
     ap.add_argument("--matvec", default="auto", choices=sorted(MATVEC),
                     help="FP32 matvec: tensor cores (3xTF32 tcgen05) or CUDA cores")
+    ap.add_argument("--compact", action="store_true",
+                    help="FP64 solves: continue on the still-active columns alone once at most half remain")
     ap.add_argument("--rows-probe", action="store_true",
                     help="time the adjoint solve, the op bodies' cache, the added mass and the mesh assembly "
                          "(one JSON line each)")

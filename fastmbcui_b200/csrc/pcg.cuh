@@ -308,6 +308,42 @@ __global__ void scatter_cols_kernel(int n, int R, int Rs, const int32_t *__restr
   dst[(size_t)i * R + idx[k]] = src[t];
 }
 
+// Column compaction of a batched PCG: the per-column state of the columns
+// idx[0 .. Rs) moves to columns 0 .. Rs of dst (the iteration temporaries
+// alpha, beta and p.t are recomputed; the stop flags start clear)
+__global__ void gather_scalars_kernel(int Rs, const int32_t *__restrict__ idx, PcgScalars src, PcgScalars dst)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k == 0) {
+    *dst.done = 0;
+    *dst.want = 0;
+  }
+  if (k >= Rs) return;
+  const int c = idx[k];
+  dst.rz[k] = src.rz[c];
+  dst.b2[k] = src.b2[c];
+  dst.thr[k] = src.thr[c];
+  dst.rr[k] = src.rr[c];
+  dst.rr_ref[k] = src.rr_ref[c];
+  dst.stall[k] = src.stall[c];
+  dst.status[k] = src.status[c];
+  dst.iters[k] = src.iters[c];
+}
+
+// ... and back: the outcome of compacted column k to column idx[k] of dst
+__global__ void scatter_scalars_kernel(int Rs, const int32_t *__restrict__ idx, PcgScalars src, PcgScalars dst)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= Rs) return;
+  const int c = idx[k];
+  dst.rz[c] = src.rz[k];
+  dst.rr[c] = src.rr[k];
+  dst.rr_ref[c] = src.rr_ref[k];
+  dst.stall[c] = src.stall[k];
+  dst.status[c] = src.status[k];
+  dst.iters[c] = src.iters[k];
+}
+
 // points (n x 3 float, stride 3) -> float4, optionally gathered by `order`
 __global__ void pack_points_kernel(int n, const float *__restrict__ src,
                                    const int32_t *__restrict__ order, float4 *__restrict__ dst)

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <type_traits>
 #include <memory>
 #include <string>
 #include <vector>
@@ -618,13 +619,14 @@ struct PcgWork {
   PcgScalars sc;
 };
 
+// PCG buffers for R columns in the given storage (vectors, block partials,
+// per-column scalars)
 template <typename T>
-static mbc_status pcg_buffers(Solver &S, int R, PcgWork<T> &w)
+static mbc_status pcg_buffers_in(Solver &S, int R, PcgWork<T> &w, DevMem &m, DevMem &part, DevMem &scal)
 {
   const size_t nv = (size_t)S.n * R, fv = (size_t)S.nf * R;
   const size_t vb = ((nv * sizeof(T)) + 255) & ~(size_t)255;
   const size_t fb = ((fv * sizeof(T)) + 255) & ~(size_t)255;
-  DevMem &m = sizeof(T) == 8 ? S.work64 : S.work32;
   MBC_TRY(m.reserve(6 * vb + fb));
   char *b = (char *)m.ptr;
   w.X = (T *)b;
@@ -636,10 +638,10 @@ static mbc_status pcg_buffers(Solver &S, int R, PcgWork<T> &w)
   w.W = (T *)(b + 6 * vb);
   const int nblk = std::max<int>(std::max<int>(cols_blocks(S), layout2d(S.n, R).grid.x), 1);
   w.part_stride = nblk;
-  MBC_TRY(S.part.reserve(sizeof(double) * (size_t)nblk * R));
-  w.part = (double *)S.part.ptr;
-  MBC_TRY(S.scal.reserve(sizeof(double) * 8 * R + sizeof(int32_t) * (3 * R + 4)));
-  double *d = (double *)S.scal.ptr;
+  MBC_TRY(part.reserve(sizeof(double) * (size_t)nblk * R));
+  w.part = (double *)part.ptr;
+  MBC_TRY(scal.reserve(sizeof(double) * 8 * R + sizeof(int32_t) * (3 * R + 4)));
+  double *d = (double *)scal.ptr;
   w.sc.rz = d;
   w.sc.b2 = d + R;
   w.sc.thr = d + 2 * R;
@@ -656,6 +658,12 @@ static mbc_status pcg_buffers(Solver &S, int R, PcgWork<T> &w)
   w.sc.stall = ii + 2 * R + 4;
   w.sc.drop2 = 0.0;
   return MBC_OK;
+}
+
+template <typename T>
+static mbc_status pcg_buffers(Solver &S, int R, PcgWork<T> &w)
+{
+  return pcg_buffers_in<T>(S, R, w, sizeof(T) == 8 ? S.work64 : S.work32, S.part, S.scal);
 }
 
 __global__ void set_status_kernel(int R, int32_t *status, int32_t *iters, int32_t *done,
@@ -694,7 +702,7 @@ template <typename T, typename LT, typename XT>
 static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, XT *x, const LT *lval, int maxit,
                           double tol, bool precond, int check_every, const int32_t *d_mask,
                           cudaStream_t st, const double *d_b2ref,
-                          const std::function<mbc_status()> *replace, int max_replace)
+                          const std::function<mbc_status()> *replace, int max_replace, bool compact = false)
 {
   // Blocks of check_every iterations have fixed kernel arguments (scalars
   // live on the device), so with S.graph a full block is captured once as a
@@ -725,6 +733,35 @@ static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, XT *x, const LT *lval
   int32_t *h_flags = S.h_flag;  // [done, want]
   if (S.profile) MBC_TRY(S.ensure_events(2 * check_every));
   int replaced = 0;
+  // Column compaction (compact, no replacement, x of the iteration's own
+  // type): once at most half of the current columns are still active, their
+  // state moves to a narrower block (ping-pong between two buffer sets) and
+  // the iteration continues on it; the stopped columns' x and outcome go back
+  // to the caller's arrays then, the rest at the end.  `cols` maps current
+  // columns to the caller's.
+  compact = compact && !replace && std::is_same<T, XT>::value;
+  PcgWork<T> *cw = &w;
+  XT *cx = x;
+  int cR = R;
+  Layout2D cL = L;
+  int cnblk2 = nblk2;
+  PcgWork<T> wc[2];
+  DevMem cwork[2], cpart[2], cscal[2], cidx;
+  int flip = 0;
+  bool compacted = false;
+  std::vector<int32_t> cols;
+  auto save_to_caller = [&]() -> mbc_status {
+    // every current column's x and outcome into the caller's arrays
+    MBC_TRY(cidx.reserve(sizeof(int32_t) * (size_t)R));
+    int32_t *d_cols = (int32_t *)cidx.ptr;
+    MBC_CK(cudaMemcpyAsync(d_cols, cols.data(), sizeof(int32_t) * cR, cudaMemcpyHostToDevice, st));
+    scatter_scalars_kernel<<<cdiv(cR, 256), 256, 0, st>>>(cR, d_cols, cw->sc, w.sc);
+    const int64_t ns = (int64_t)S.n * cR;
+    scatter_cols_kernel<XT><<<cdiv(ns, 256), 256, 0, st>>>(S.n, R, cR, d_cols, cx, x);
+    S.launches += 2;
+    MBC_CKL();
+    return MBC_OK;
+  };
   for (int it = 0; it < maxit; it += check_every) {
     const int kmax = std::min(check_every, maxit - it);
     // (the captured block holds kernel launches only: the unpreconditioned
@@ -738,26 +775,26 @@ static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, XT *x, const LT *lval
     if (use_graph && !graph.exec) MBC_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
     for (int k = 0; k < kmax && !(use_graph && graph.exec && graph_launches > 0); ++k) {
       if (precond) {
-        precond_lt_kernel<T, LT><<<L.grid, L.block, 0, st>>>(S.n, R, S.d_lptr(), S.d_lind(), lval,
-                                                              w.Rv, w.U, w.sc.done);
-        precond_l_kernel<T, LT><<<L.grid, L.block, L.smem, st>>>(S.n, R, S.d_rptr(), S.d_rcol(),
-                                                                 S.d_rmap(), lval, w.U, w.Z, w.Rv,
-                                                                 w.part, w.sc.done);
+        precond_lt_kernel<T, LT><<<cL.grid, cL.block, 0, st>>>(S.n, cR, S.d_lptr(), S.d_lind(), lval,
+                                                                cw->Rv, cw->U, cw->sc.done);
+        precond_l_kernel<T, LT><<<cL.grid, cL.block, cL.smem, st>>>(S.n, cR, S.d_rptr(), S.d_rcol(),
+                                                                   S.d_rmap(), lval, cw->U, cw->Z, cw->Rv,
+                                                                   cw->part, cw->sc.done);
       } else {
-        MBC_CK(cudaMemcpyAsync(w.Z, w.Rv, sizeof(T) * (size_t)S.n * R, cudaMemcpyDeviceToDevice, st));
-        dot_partial_kernel<T><<<L.grid, L.block, L.smem, st>>>(S.n, R, w.Rv, w.Z, w.part);
+        MBC_CK(cudaMemcpyAsync(cw->Z, cw->Rv, sizeof(T) * (size_t)S.n * cR, cudaMemcpyDeviceToDevice, st));
+        dot_partial_kernel<T><<<cL.grid, cL.block, cL.smem, st>>>(S.n, cR, cw->Rv, cw->Z, cw->part);
       }
-      reduce_kernel<<<1, 1024, 0, st>>>(nblk2, R, w.part, RED_BETA, w.sc, nullptr);
-      update_p_kernel<T><<<L.grid, L.block, 0, st>>>(S.n, R, w.sc.beta, w.sc.status, w.Z, w.Pv,
-                                                      w.sc.done);
+      reduce_kernel<<<1, 1024, 0, st>>>(cnblk2, cR, cw->part, RED_BETA, cw->sc, nullptr);
+      update_p_kernel<T><<<cL.grid, cL.block, 0, st>>>(S.n, cR, cw->sc.beta, cw->sc.status, cw->Z, cw->Pv,
+                                                        cw->sc.done);
       if (S.profile) MBC_CK(cudaEventRecord(S.events[2 * k], st));
-      launch_rows<T>(S, R, w.Pv, w.W, w.sc.done, st);
-      const int nb = launch_cols<T>(S, R, w.W, w.Tt, w.Pv, w.part, w.sc.done, st);
+      launch_rows<T>(S, cR, cw->Pv, cw->W, cw->sc.done, st);
+      const int nb = launch_cols<T>(S, cR, cw->W, cw->Tt, cw->Pv, cw->part, cw->sc.done, st);
       if (S.profile) MBC_CK(cudaEventRecord(S.events[2 * k + 1], st));
-      reduce_kernel<<<1, 1024, 0, st>>>(nb, R, w.part, RED_ALPHA, w.sc, nullptr);
-      update_xr_kernel<T, XT><<<L.grid, L.block, L.smem, st>>>(S.n, R, w.sc.alpha, w.Pv, w.Tt, x,
-                                                               w.Rv, w.part, w.sc.done);
-      reduce_kernel<<<1, 1024, 0, st>>>(nblk2, R, w.part, RED_CHECK, w.sc, nullptr);
+      reduce_kernel<<<1, 1024, 0, st>>>(nb, cR, cw->part, RED_ALPHA, cw->sc, nullptr);
+      update_xr_kernel<T, XT><<<cL.grid, cL.block, cL.smem, st>>>(S.n, cR, cw->sc.alpha, cw->Pv, cw->Tt, cx,
+                                                                 cw->Rv, cw->part, cw->sc.done);
+      reduce_kernel<<<1, 1024, 0, st>>>(cnblk2, cR, cw->part, RED_CHECK, cw->sc, nullptr);
       S.launches += precond ? 7 : 6;  // the matvec pair counts itself
     }
     if (use_graph && !graph.exec) {
@@ -771,7 +808,7 @@ static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, XT *x, const LT *lval
       MBC_CK(cudaGraphLaunch(graph.exec, st));
     }
     MBC_CKL();
-    MBC_CK(cudaMemcpyAsync(h_flags, w.sc.done, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    MBC_CK(cudaMemcpyAsync(h_flags, cw->sc.done, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     MBC_CK(cudaStreamSynchronize(st));
     if (S.profile) {
       // iterations after the last active column stopped exit at once; they
@@ -792,7 +829,60 @@ static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, XT *x, const LT *lval
       MBC_CK(cudaStreamSynchronize(st));
       if (h_flags[0]) break;
     }
+    if constexpr (std::is_same<T, XT>::value) {
+      if (compact && it + check_every < maxit) {
+        std::vector<int32_t> stat(cR);
+        MBC_CK(cudaMemcpyAsync(stat.data(), cw->sc.status, sizeof(int32_t) * cR, cudaMemcpyDeviceToHost, st));
+        MBC_CK(cudaStreamSynchronize(st));
+        std::vector<int32_t> act;
+        for (int c = 0; c < cR; ++c)
+          if (stat[c] == COL_ACTIVE) act.push_back(c);
+        const int A = (int)act.size();
+        if (A > 0 && 2 * A <= cR && cR - A >= 8) {
+          if (!compacted) {
+            cols.resize(R);
+            for (int c = 0; c < R; ++c) cols[c] = c;
+          } else {
+            MBC_TRY(save_to_caller());
+          }
+          PcgWork<T> &nw = wc[flip];
+          MBC_TRY(pcg_buffers_in<T>(S, A, nw, cwork[flip], cpart[flip], cscal[flip]));
+          MBC_TRY(cidx.reserve(sizeof(int32_t) * (size_t)R));
+          int32_t *d_act = (int32_t *)cidx.ptr;
+          MBC_CK(cudaMemcpyAsync(d_act, act.data(), sizeof(int32_t) * A, cudaMemcpyHostToDevice, st));
+          const int64_t ns = (int64_t)S.n * A;
+          gather_cols_kernel<T><<<cdiv(ns, 256), 256, 0, st>>>(S.n, cR, A, d_act, cx, nw.X);
+          gather_cols_kernel<T><<<cdiv(ns, 256), 256, 0, st>>>(S.n, cR, A, d_act, cw->Rv, nw.Rv);
+          gather_cols_kernel<T><<<cdiv(ns, 256), 256, 0, st>>>(S.n, cR, A, d_act, cw->Pv, nw.Pv);
+          gather_scalars_kernel<<<cdiv(A, 256), 256, 0, st>>>(A, d_act, cw->sc, nw.sc);
+          S.launches += 4;
+          MBC_CKL();
+          nw.sc.maxit = cw->sc.maxit;
+          nw.sc.tol2 = cw->sc.tol2;
+          nw.sc.drop2 = cw->sc.drop2;
+          std::vector<int32_t> ncols(A);
+          for (int k = 0; k < A; ++k) ncols[k] = cols[act[k]];
+          cols.swap(ncols);
+          // the next block waits for the gathers (same stream); the source
+          // buffers are not touched again
+          MBC_CK(cudaStreamSynchronize(st));
+          cw = &nw;
+          cx = nw.X;
+          cR = A;
+          cL = layout2d(S.n, A);
+          cnblk2 = (int)cL.grid.x;
+          flip ^= 1;
+          compacted = true;
+          if (graph.exec) {  // the captured block has the old width baked in
+            cudaGraphExecDestroy(graph.exec);
+            graph.exec = nullptr;
+            graph_launches = 0;
+          }
+        }
+      }
+    }
   }
+  if (compacted) MBC_TRY(save_to_caller());
   S.replacements = replaced;
   return MBC_OK;
 }
@@ -929,7 +1019,8 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
   PcgWork<T> w;
   MBC_TRY(pcg_buffers<T>(*this, R, w));
   // F (forward) lives in fbuf (T, nf x R); with the INT8 FP64 operator the
-  // adjoint right-hand side b is kept there too (n x R), for the replacements
+  // adjoint right-hand side b is kept there too (n x R), for the residual
+  // checks after the PCG
   DevMem &fm = sizeof(T) == 8 ? fbuf64 : fbuf32;
   const bool oz = sizeof(T) == 8 && use_oz(*this);
   if (!adjoint) {
@@ -967,40 +1058,81 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
     MBC_TRY(col_norms2_dev<T>(*this, R, bvec, (double *)b2ref.ptr, st));
     b2 = (const double *)b2ref.ptr;
   }
-  // The INT8 FP64 operator carries a ~1e-10 relative error, so the recursive
-  // residual drifts from b - K^T K x by about that much per hundred
-  // iterations: columns converge only on residuals recomputed with the same
-  // operator (replacement mode), which keeps p and the Krylov information.
-  std::function<mbc_status()> replace_fn = [&]() -> mbc_status {
-    const Layout2D L = layout2d(n, R);
-    if (adjoint) {
-      launch_rows<T>(*this, R, w.X, w.W, nullptr, st);
-      launch_cols<T>(*this, R, w.W, w.Tt, nullptr, nullptr, nullptr, st);
-      sub_kernel<T><<<cdiv(nv, 256), 256, 0, st>>>(nv, (const T *)fm.ptr, w.Tt, w.Rv);
-      ++launches;
-    } else {
-      residual<T>(*this, R, (const T *)fm.ptr, w.X, w.W, w.Rv, st);
-    }
-    dot_partial_kernel<T><<<L.grid, L.block, L.smem, st>>>(n, R, w.Rv, w.Rv, w.part);
-    reduce_kernel<<<1, 1024, 0, st>>>((int)L.grid.x, R, w.part, RED_REPLACE, w.sc, nullptr);
-    launches += 2;
-    MBC_CKL();
-    return MBC_OK;
-  };
-  if (oz) w.sc.drop2 = 1e-300;  // replace only where a column would stop
+  const bool compact = o.compact != 0;
   if (precision == MBC_F64)
     MBC_TRY((run_pcg<T, double, T>(*this, R, w, w.X, (const double *)lval.ptr, o.max_iters, o.tol,
                                    o.precondition != 0, std::max(1, o.check_every), nullptr, st, b2,
-                                   oz ? &replace_fn : nullptr, oz ? 64 : 0)));
+                                   nullptr, 0, compact)));
   else
     MBC_TRY((run_pcg<T, float, T>(*this, R, w, w.X, (const float *)lval.ptr, o.max_iters, o.tol,
                                   o.precondition != 0, std::max(1, o.check_every), nullptr, st, b2,
-                                  nullptr, 0)));
+                                  nullptr, 0, compact)));
   std::vector<int32_t> status, iters;
   std::vector<double> rel;
   MBC_TRY(collect<T>(*this, R, w, status, iters, rel, st));
-  for (int c = 0; c < R; ++c)
-    if (status[c] == COL_STAGNANT) status[c] = COL_MAXIT;
+  if constexpr (sizeof(T) == 8) {
+    if (oz) {
+      // The INT8 FP64 operator carries a ~1e-10 relative error, so the
+      // recursive residual can end slightly above tol once recomputed with
+      // the same operator (1.3e-8 for 1e-8 after ~270 iterations in
+      // emulation).  Every column is decided on that recomputed residual, and
+      // those above tol restart from where they stand, at most twice.
+      T *bvec = w.Tt;
+      if (adjoint) MBC_CK(cudaMemcpyAsync(bvec, fm.ptr, sizeof(T) * nv, cudaMemcpyDeviceToDevice, st));
+      else launch_cols<T>(*this, R, (const T *)fm.ptr, bvec, nullptr, nullptr, nullptr, st);
+      MBC_CKL();
+      std::vector<double> nb;
+      MBC_TRY(col_norms2<T>(*this, R, bvec, nb, st));
+      for (int pass = 0; pass < 3; ++pass) {
+        if (adjoint) {
+          launch_rows<T>(*this, R, w.X, w.W, nullptr, st);
+          launch_cols<T>(*this, R, w.W, w.Z, nullptr, nullptr, nullptr, st);
+          sub_kernel<T><<<cdiv(nv, 256), 256, 0, st>>>(nv, (const T *)fm.ptr, w.Z, w.Rv);
+          ++launches;
+        } else {
+          residual<T>(*this, R, (const T *)fm.ptr, w.X, w.W, w.Rv, st);
+        }
+        MBC_CKL();
+        std::vector<double> nr;
+        MBC_TRY(col_norms2<T>(*this, R, w.Rv, nr, st));
+        std::vector<int32_t> pol;
+        for (int c = 0; c < R; ++c) {
+          rel[c] = nb[c] < 1e-16 ? 0.0 : std::sqrt(nr[c] / nb[c]);
+          if (status[c] == COL_BREAKDOWN) continue;
+          status[c] = rel[c] <= o.tol ? COL_OK : COL_MAXIT;
+          if (status[c] == COL_MAXIT) pol.push_back(c);
+        }
+        if (pol.empty() || pass == 2) break;
+        const int Rs = (int)pol.size();
+        PcgWork<T> ws;
+        DevMem wmem, wpart, wscal, widx;
+        MBC_TRY(pcg_buffers_in<T>(*this, Rs, ws, wmem, wpart, wscal));
+        const size_t ib = ((sizeof(int32_t) * Rs) + 15) & ~(size_t)15;
+        MBC_TRY(widx.reserve(ib + sizeof(double) * Rs));
+        int32_t *d_idx = (int32_t *)widx.ptr;
+        double *d_b2s = (double *)((char *)widx.ptr + ib);
+        std::vector<double> b2s(Rs);
+        for (int k = 0; k < Rs; ++k) b2s[k] = nb[pol[k]];
+        MBC_CK(cudaMemcpyAsync(d_idx, pol.data(), sizeof(int32_t) * Rs, cudaMemcpyHostToDevice, st));
+        MBC_CK(cudaMemcpyAsync(d_b2s, b2s.data(), sizeof(double) * Rs, cudaMemcpyHostToDevice, st));
+        const int64_t ns = (int64_t)n * Rs;
+        gather_cols_kernel<T><<<cdiv(ns, 256), 256, 0, st>>>(n, R, Rs, d_idx, w.X, ws.X);
+        gather_cols_kernel<T><<<cdiv(ns, 256), 256, 0, st>>>(n, R, Rs, d_idx, w.Rv, ws.Rv);
+        launches += 2;
+        MBC_CKL();
+        MBC_TRY((run_pcg<T, double, T>(*this, Rs, ws, ws.X, (const double *)lval.ptr, o.max_iters, o.tol,
+                                       o.precondition != 0, std::max(1, o.check_every), nullptr, st, d_b2s,
+                                       nullptr, 0, compact)));
+        std::vector<int32_t> it2(Rs);
+        MBC_CK(cudaMemcpyAsync(it2.data(), ws.sc.iters, sizeof(int32_t) * Rs, cudaMemcpyDeviceToHost, st));
+        scatter_cols_kernel<T><<<cdiv(ns, 256), 256, 0, st>>>(n, R, Rs, d_idx, ws.X, w.X);
+        ++launches;
+        MBC_CKL();
+        MBC_CK(cudaStreamSynchronize(st));
+        for (int k = 0; k < Rs; ++k) iters[pol[k]] += it2[k];
+      }
+    }
+  }
   permute_out<T>(*this, R, w.X, X, x_dt, st);
   MBC_CKL();
   MBC_TRY(finish_stats(R, status, iters, rel, stats, iters_host));

@@ -188,6 +188,9 @@ typedef struct {
   int32_t profile;       /* 1 = time the matvec kernels with CUDA events on `stream` */
   int32_t graph;         /* 1 = replay blocks of check_every PCG iterations as a CUDA graph
                             (captured on the first full block; ignored with profile) */
+  int32_t compact;       /* 1 = once at most half of the columns are still iterating (and at
+                            least 8 have stopped), continue with those columns alone, so the
+                            matvecs carry only them (FP64 and plain FP32 solves) */
 } mbc_solve_options;
 
 typedef struct {

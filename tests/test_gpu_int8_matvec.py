@@ -12,7 +12,7 @@ the scheme's worst-case error; kc = 2048-wide chunk length):
     kernels recompute it), at most 10 % + one check block more iterations
     than the FP64 kernels, fitted flux within 1e-6 of theirs (relative to |F|).
 
-The tests that run the INT8 kernels are skipped unless MBC_INT8_GPU=1: they
+The tests that run the INT8 kernels are skipped unless MBC_FIRST_GPU_RUN=1: they
 wait for their first supervised GPU run.
 """
 import os
@@ -26,8 +26,8 @@ from fastmbcui_b200 import _lib
 from fastmbcui_b200 import scenes as S
 
 pytestmark = pytest.mark.gpu
-int8_run = pytest.mark.skipif(os.environ.get("MBC_INT8_GPU") != "1",
-                              reason="INT8 matvec kernels: first supervised GPU run pending (MBC_INT8_GPU=1)")
+int8_run = pytest.mark.skipif(os.environ.get("MBC_FIRST_GPU_RUN") != "1",
+                              reason="INT8 matvec kernels: first supervised GPU run pending (MBC_FIRST_GPU_RUN=1)")
 
 torch = pytest.importorskip("torch")
 CHUNK = 2048
