@@ -1281,7 +1281,7 @@ mbc_status Solver::solve_mixed(int R, const void *rhs, int32_t rhs_dt, void *X, 
     MBC_TRY((run_pcg<double, float, double>(*this, Rs, w64, w64.X, (const float *)lval.ptr,
                                             o.max_iters, o.tol, o.precondition != 0,
                                             std::max(1, o.check_every), nullptr, st, d_b2s, nullptr,
-                                            0)));
+                                            0, o.compact != 0)));
     std::vector<int32_t> it64(Rs);
     MBC_CK(cudaMemcpyAsync(it64.data(), w64.sc.iters, sizeof(int32_t) * Rs, cudaMemcpyDeviceToHost, st));
     scatter_cols_kernel<double><<<cdiv(ns, 256), 256, 0, st>>>(n, R, Rs, d_idx, w64.X, Xd);

@@ -190,7 +190,8 @@ typedef struct {
                             (captured on the first full block; ignored with profile) */
   int32_t compact;       /* 1 = once at most half of the columns are still iterating (and at
                             least 8 have stopped), continue with those columns alone, so the
-                            matvecs carry only them (FP64 and plain FP32 solves) */
+                            matvecs carry only them (FP64 and plain FP32 solves, and the
+                            FP64 polish of MBC_F32 solves) */
 } mbc_solve_options;
 
 typedef struct {
