@@ -207,7 +207,8 @@ def run_trajectory(args):
     coords = [(t(sc.x), t(sc.nx), t(sc.y)) for sc in scenes]  # inputs resident in HBM
     Fm = [t(sc.rhs()) for sc in scenes]
     R = Fm[0].shape[1]
-    opts = dict(tol=1e-8, max_iters=args.max_iters, max_refine=64, inner_tol=1e-2, check_every=8)
+    opts = dict(tol=1e-8, max_iters=args.max_iters, max_refine=64, inner_tol=1e-2, check_every=8,
+                compact=int(args.compact))
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     # learned warm start: the trained network and the bodies' isolated
     # solutions (a per-shape cache computed once, outside the timed steps)
@@ -360,7 +361,7 @@ def run_trajectory(args):
                                   "previous": "previous step's strengths", "cold": "x0 = 0"}[args.warm],
                    "steps_run": f"{args.warmup} warm-up + {args.steps} timed",
                    "plan_every": args.plan_every, "solver": args.solver, "fp64_matvec": args.fp64_matvec,
-                   "compact": bool(args.compact and args.solver == "fp64"),
+                   "compact": bool(args.compact) and args.solver != "flexible",
                    "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas{world}"},
         "e2e": {"value": round(e2e, 5), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h),
@@ -640,7 +641,8 @@ def run_ours(args):
     x, nx, y, Fd = t(sc.x), t(sc.nx), t(sc.y), t(Fm)
     solver = F.Solver(plan, x=x, nx=nx, y=y, coef=sc.coef, precision=F.MBC_F32)
     solver.set_matvec(MATVEC[args.matvec]).set_fp64_matvec(args.fp64_matvec)
-    opts = dict(tol=1e-8, max_iters=args.max_iters, max_refine=64, inner_tol=1e-2, check_every=8)
+    opts = dict(tol=1e-8, max_iters=args.max_iters, max_refine=64, inner_tol=1e-2, check_every=8,
+                compact=int(args.compact))
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
 
     def step(profile=0):
