@@ -582,7 +582,7 @@ def run_uneven(args):
     dev = torch.device("cuda", 0)
     scs = S.uneven_batch(args.scenes, first_seed=3)
     t = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
-    plans = [F.Plan(sc.y, sc.rho, sc.lam, sc.max_super) for sc in scs]
+    plans = F.plan_many([(sc.y, sc.rho, sc.lam, sc.max_super) for sc in scs])
     data = [(t(sc.x), t(sc.nx), t(sc.y), t(sc.rhs())) for sc in scs]
     fp64 = args.solver == "fp64"
     opts = dict(out_dtype=torch.float64 if fp64 else torch.float32, tol=1e-8, max_iters=args.max_iters,

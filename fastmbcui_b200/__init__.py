@@ -16,7 +16,8 @@ from ._lib import (MBC_F32, MBC_F64, MBC_FP64_MATVEC_INT8, MBC_FP64_MATVEC_SIMT,
                    MBC_OP_DENSE, MBC_OP_POINT_KERNEL, MBC_SCHED_BATCHED, MBC_SCHED_PER_RHS, MbcError,
                    check, ptr)
 
-__all__ = ["Plan", "Solver", "MbcError", "load", "MBC_F32", "MBC_F64", "MBC_SCHED_BATCHED",
+__all__ = ["Plan", "Solver", "MbcError", "load", "plan_many", "solve_many", "MBC_F32", "MBC_F64",
+           "MBC_SCHED_BATCHED",
            "MBC_SCHED_PER_RHS", "MBC_MATVEC_AUTO", "MBC_MATVEC_SIMT", "MBC_MATVEC_TENSOR",
            "MBC_FP64_MATVEC_SIMT", "MBC_FP64_MATVEC_INT8"]
 
@@ -257,6 +258,22 @@ class Solver:
                                     None if frc is None else frc.ctypes.data, self._sp()),
               "mbc_added_mass")
         return (Mf, frc) if accel is not None else Mf
+
+
+def plan_many(specs, threads=None):
+    """Host plans of many scenes at once: specs = [(points, rho, lam,
+    max_super), ...], planned on a thread pool (the plan code keeps no shared
+    state and the binding releases the interpreter lock during the call).
+    Returns the Plans in input order, identical to planning them one by one."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+
+    specs = list(specs)
+    if not specs:
+        return []
+    workers = threads or min(len(specs), os.cpu_count() or 1)
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        return list(ex.map(lambda a: Plan(*a), specs))
 
 
 def solve_many(solvers, Fs, X0s=None, threads=None, factor=True, **opts):
