@@ -1696,6 +1696,7 @@ extern "C" void mbc_solve_default_options(mbc_solve_options *o)
   o->true_residual = 0;
   o->profile = 0;
   o->graph = 0;
+  o->compact = 0;
 }
 
 static mbc_status check_solve_args(mbc_solver *s, int32_t R, const void *in, int32_t in_dt, void *X,

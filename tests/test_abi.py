@@ -56,3 +56,60 @@ def test_context_lifecycle_without_gpu():
     assert s == _lib.MBC_BAD_ARG
     assert b"MinvF_float first" in L.mbc_last_error()
     assert L.mbc_context_destroy(h) == 0
+
+
+def test_default_options_set_every_field():
+    """mbc_solve_default_options writes every field of mbc_solve_options, so a
+    C caller's struct on the stack holds no garbage afterwards (compact, the
+    newest field, included)."""
+    import ctypes as C
+
+    from fastmbcui_b200 import _lib, load
+
+    o = _lib.SolveOptions()
+    C.memset(C.byref(o), 0xFF, C.sizeof(o))
+    load().mbc_solve_default_options(C.byref(o))
+    want = {"max_iters": 1000, "tol": 1e-8, "schedule": 0, "precondition": 1, "max_refine": 64,
+            "inner_tol": 1e-2, "check_every": 8, "true_residual": 0, "profile": 0, "graph": 0, "compact": 0}
+    assert {k for k, _ in _lib.SolveOptions._fields_} == set(want)
+    for k, v in want.items():
+        assert getattr(o, k) == v, k
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """The ctypes mirrors of the header's structs have the header's field
+    order, offsets and sizes (a C program built against include/mbc.h prints
+    them)."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        import pytest
+
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    mirrors = {"mbc_plan_options": _lib.PlanOptions, "mbc_plan_info": _lib.PlanInfo,
+               "mbc_operator": _lib.Operator, "mbc_solve_options": _lib.SolveOptions,
+               "mbc_solve_stats": _lib.SolveStats}
+    cfield = {"lambda_": "lambda"}  # Python keywords carry a trailing underscore in the mirrors
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "mbc.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'  printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'  printf("{cname} {f} %zu\\n", offsetof({cname}, {cfield.get(f, f)}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c99", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {}
+    for ln in out:
+        if ln:
+            name, field, val = ln.split()
+            got[(name, field)] = int(val)
+    for cname, py in mirrors.items():
+        assert got[(cname, "sizeof")] == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
