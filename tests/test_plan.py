@@ -85,3 +85,27 @@ def test_errors():
         F.Plan(np.zeros((0, 3)))
     with pytest.raises(F.MbcError):
         F.Plan(np.random.default_rng(0).random((10, 3)), rho=-1.0)
+
+
+def test_boxes_above_floor_plan():
+    """The large configuration (N = 200000, rho 4, supernodes capped at 512):
+    the floor's 400 x 250 regular grid is full of exactly equal distances, so
+    the maximin tie-breaking decides the ordering; the product's plan must
+    still equal the oracle's bit for bit."""
+    sc = S.large_scene()
+    p, _ = assert_same(sc.y, rho=sc.rho, lam=sc.lam, max_super=sc.max_super)
+    assert p.info.n == 200000
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build (oracle/_ref) not present")
+def test_boxes_above_floor_order_matches_reference():
+    """On the same points the reference's own maximin ordering and radius
+    search (src/maxmin.h, src/nanoflann.hpp built into oracle/_ref) agree
+    with the oracle's, at the configuration's rho = 4."""
+    sc = S.large_scene()
+    P, s = O.order(sc.y)
+    Pr, sr = O.ref_order(sc.y)
+    assert np.array_equal(P, Pr) and np.array_equal(s, sr)
+    ptr, ind = O.pattern(sc.y, P, s, sc.rho)
+    ptr2, ind2 = O.ref_pattern(sc.y, Pr, sr, sc.rho)
+    assert np.array_equal(ptr, ptr2) and np.array_equal(ind, ind2)
