@@ -47,3 +47,21 @@ def test_compacted_solve_matches(fp64_matvec):
     rel = np.linalg.norm(op.KT(Fm - op.K(X1)), axis=0) / np.linalg.norm(b, axis=0)
     assert rel.max() <= 1.05e-8, rel
     assert np.linalg.norm(op.K(X1) - op.K(X0)) / np.linalg.norm(Fm) < 1e-8
+
+
+def test_compacted_polish_of_the_mixed_solve():
+    """MBC_F32 solves: the FP64 polish compacts too; every column still ends
+    at an FP64 true residual <= 1.05e-8, and the flux matches the
+    uncompacted solve within 1e-7 of |F|."""
+    sc = S.ellipsoids_scene(3, 1000, seed=17)
+    plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
+    s = F.Solver(plan, x=_dev(sc.x), nx=_dev(sc.nx), y=_dev(sc.y), coef=sc.coef, precision=F.MBC_F32).factor()
+    Fm = sc.rhs()
+    X0, _ = s.solve(_dev(Fm), out_dtype=torch.float64, tol=1e-8, max_iters=3000, check_every=4)
+    X1, st1 = s.solve(_dev(Fm), out_dtype=torch.float64, tol=1e-8, max_iters=3000, check_every=4, compact=1)
+    X0, X1 = X0.cpu().numpy(), X1.cpu().numpy()
+    op = O.Op.from_scene(sc)
+    b = op.KT(Fm)
+    rel = np.linalg.norm(op.KT(Fm - op.K(X1)), axis=0) / np.linalg.norm(b, axis=0)
+    assert rel.max() <= 1.05e-8, (rel, st1)
+    assert np.linalg.norm(op.K(X1) - op.K(X0)) / np.linalg.norm(Fm) < 1e-7
