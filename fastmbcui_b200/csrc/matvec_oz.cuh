@@ -29,8 +29,8 @@
 //     2^(a_row + b_col - kScaleShift).
 // Measured in emulation on the normal equations of an MFS scene: operator
 // error 1.6e-10 relative at the solution, and PCG with this operator in both
-// directions reaches the FP64 true residual of 1e-8 (after one residual
-// replacement) in 4 % more iterations than the FP64 operator.
+// directions reaches the FP64 true residual of 1e-8 (after one restart from
+// the recomputed residual) in 4 % more iterations than the FP64 operator.
 //
 // G is evaluated with PointKernel<double>::eval, the function the FP64
 // CUDA-core kernels use, so the digits encode the same FP64 values.  G does
