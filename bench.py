@@ -393,6 +393,10 @@ def run_trajectory(args):
 # DRAM bytes (read + write) per launch of the tensor-core matvec at N = Nf =
 # 64000, R = 192, from one ncu capture of the K / K^T probe
 TC_TRAFFIC_BYTES = 442e6
+# the same for the FP64 CUDA-core matvec (pk_rows_kernel<double>, 109.5 MB read
+# + 63.2 MB written at R = 192); its traffic is the vector block in and out,
+# so a launch carrying R columns moves about R / 192 of it
+FP64_TRAFFIC_BYTES_R192 = 172.7e6
 
 
 def _matvec_roofline(st, nf, n, R, matvec, fp64_matvec="simt"):
@@ -445,8 +449,11 @@ def _matvec_roofline(st, nf, n, R, matvec, fp64_matvec="simt"):
                                    f"HBM {hbm} GB/s (of measured)",
                     "fp64_matvec": fp64, "tensor_matvec": tc}
     ach, ms = (a64, ms64) if dom64 else (a32, ms32)
+    if fp64_matvec != "int8" and nf == n == 64000:
+        fp64["traffic"] = round(FP64_TRAFFIC_BYTES_R192 * R64 / 192)
+        fp64["traffic_source"] = "ncu capture at R = 192 (profiles/pk_fp64_matvec_ellipsoids32.md), scaled by columns"
     return {"bound": "tensor", "achieved": round(ach, 2), "peak": bf16, "unit": "TFLOP/s",
-            "frac": round(ach / bf16, 4), "traffic": None if dom64 else tc["traffic"],
+            "frac": round(ach / bf16, 4), "traffic": fp64.get("traffic") if dom64 else tc["traffic"],
             "kernel": fp64["kernel"] if dom64 else tc["kernel"], "launch_ms": round(ms, 3),
             "peak_source": f"bf16 dense, {src} (of measured); the FP64 kernel's own ceiling is the "
                            f"FP64 pipe (37 TFLOP/s nominal, no measured figure)",
