@@ -258,8 +258,9 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32])
 
 // The B image: for each k-step ks, [hi tile | lo tile], each np rows x 128 B
 // laid out by sw128; element (r, k) = vin[(32 ks + k) * R + r], zero outside.
-// One thread per (k-step, row r, group of 4 k).
-__global__ void pack_b_kernel(const float *__restrict__ vin, int K_total, int R, int np, int nks,
+// One thread per (k-step, row r, group of 4 k).  Internal linkage: several
+// translation units include this header.
+static __global__ void pack_b_kernel(const float *__restrict__ vin, int K_total, int R, int np, int nks,
                               uint4 *__restrict__ img, const int32_t *__restrict__ done)
 {
   if (done && *done) return;

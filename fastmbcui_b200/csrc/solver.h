@@ -109,3 +109,8 @@ int launch_cols(const Solver &S, int R, const T *w, T *t, const T *pdot, double 
                 const int32_t *done, cudaStream_t st);
 
 }  // namespace mbc
+
+// The C handle behind mbc_solver.
+struct mbc_solver {
+  mbc::Solver s;
+};
