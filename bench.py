@@ -238,10 +238,17 @@ def run_trajectory(args):
             return 2.0 * hist[-1] - hist[-2]
         return hist[-1]
 
-    out_dt = torch.float64 if args.solver == "fp64" else torch.float32
+    out_dt = torch.float64 if args.solver in ("fp64", "mixed64") else torch.float32
 
     def solve_scene(plan, x, nx, y, Fk, X0, profile=0):
         """One step's factor and solve through the selected path."""
+        if args.solver == "mixed64":
+            # FP32 factor (FP64 retry of cancelling supernodes) preconditioning
+            # an FP64 PCG whose matvecs follow --fp64-matvec
+            s = F.Solver(plan, x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F32)
+            s.set_fp64_matvec(args.fp64_matvec).factor()
+            return s.solve(Fk, X0=X0, out_dtype=torch.float64, profile=profile, tol=1e-8,
+                           max_iters=args.max_iters, check_every=8, compact=int(args.compact), fp64_recursion=1)
         if args.solver == "fp64":
             # FP64 PCG with the FP64 factor; with --fp64-matvec int8 its
             # matvecs run on the INT8 tensor cores
@@ -354,6 +361,7 @@ def run_trajectory(args):
                    "Nf": base.nf, "R": R, "rho": base.rho, "lambda": base.lam, "tol": 1e-8,
                    "precision": {"flexible": "FP64 flexible CG around FP32 PCG",
                                  "fp64": "FP64 PCG, FP64 factor",
+                                 "mixed64": "FP64 PCG, FP32 factor",
                                  "mixed": "mixed FP32/FP64 residual replacement"}[args.solver],
                    "schedule": "batched",
                    "warm_start": {"learned": "previous step + MLP correction (3x256, BF16 weights)",
@@ -910,7 +918,7 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=572)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scenes", type=int, default=8, help="uneven workload: scenes in the sample")
-    ap.add_argument("--solver", default="mixed", choices=["mixed", "flexible", "fp64"],
+    ap.add_argument("--solver", default="mixed", choices=["mixed", "flexible", "fp64", "mixed64"],
                     help="trajectory and uneven: residual-replacement mixed PCG, FP64 flexible CG around the "
                          "FP32 PCG (trajectory), or FP64 PCG (pair with --fp64-matvec int8)")
     ap.add_argument("--inner-iters", type=int, default=40, help="flexible solver: FP32 iterations per outer step")

@@ -45,7 +45,7 @@ class SolveOptions(C.Structure):
     _fields_ = [("max_iters", C.c_int32), ("tol", C.c_double), ("schedule", C.c_int32),
                 ("precondition", C.c_int32), ("max_refine", C.c_int32), ("inner_tol", C.c_double),
                 ("check_every", C.c_int32), ("true_residual", C.c_int32), ("profile", C.c_int32),
-                ("graph", C.c_int32), ("compact", C.c_int32)]
+                ("graph", C.c_int32), ("compact", C.c_int32), ("fp64_recursion", C.c_int32)]
 
 
 class SolveStats(C.Structure):

@@ -36,7 +36,9 @@ __device__ __align__(256) static float4 g_noalloc_scratch[kSlots];
 
 // Device address of g_noalloc_scratch per device.  In host code the symbol is
 // only a handle for the runtime, so the address is looked up, once per device,
-// with that device current.
+// with that device current.  The addresses stay cached for the process:
+// cudaDeviceReset unloads the module, after which this entry point must not
+// be called again in the same process.
 std::mutex g_mu;
 float4 *g_addr[kMaxDevices] = {};
 
@@ -74,7 +76,7 @@ template <int RC, int TI>
 void rows(const float4 *x4, const float4 *n4, int nf, const float4 *y4, int n, float coef, int R,
           const float *v, float *w, cudaStream_t st)
 {
-  dim3 grid((unsigned)((nf + TI - 1) / TI), (unsigned)((R + RC - 1) / RC));
+  dim3 grid((unsigned)((nf + TI - 1) / TI), (unsigned)(((int64_t)R + RC - 1) / RC));
   mbc::pk_rows_kernel<float, RC, TI, kTjRows><<<grid, TI, 0, st>>>(x4, n4, nf, y4, n, v, R, coef, w, R, R,
                                                                   nullptr);
 }
@@ -83,7 +85,7 @@ template <int RC, int TI>
 void cols(const float4 *x4, const float4 *n4, int nf, const float4 *y4, int n, float coef, int R,
           const float *w, float *t, cudaStream_t st)
 {
-  dim3 grid((unsigned)((n + TI - 1) / TI), (unsigned)((R + RC - 1) / RC));
+  dim3 grid((unsigned)((n + TI - 1) / TI), (unsigned)(((int64_t)R + RC - 1) / RC));
   mbc::pk_cols_kernel<float, RC, TI, kTjCols><<<grid, TI, 0, st>>>(x4, n4, nf, y4, n, w, R, coef, t, R, R,
                                                                   nullptr, nullptr, nullptr);
 }
@@ -110,7 +112,20 @@ extern "C" mbc_status mbc_point_apply_noalloc(int32_t transpose, int32_t nf, int
     return fail(MBC_BAD_ARG, "mbc_point_apply_noalloc: 2*nf + n = " + std::to_string(2 * (int64_t)nf + n) +
                                  " points exceed the static scratch (2*ceil16(nf) + ceil16(n) <= " +
                                  std::to_string(kSlots) + " float4 slots, 4 MiB)");
-  if ((R + 31) / 32 > 65535) return fail(MBC_BAD_ARG, "mbc_point_apply_noalloc: R above 2,097,120");
+  if (((int64_t)R + 31) / 32 > 65535) return fail(MBC_BAD_ARG, "mbc_point_apply_noalloc: R above 2,097,120");
+  // the kernels read `in` while other blocks write `out` (both __restrict__):
+  // an in-place or overlapping call would silently return wrong values
+  const int64_t in_bytes = (int64_t)(transpose ? nf : n) * R * (int64_t)sizeof(float);
+  const int64_t out_bytes = (int64_t)(transpose ? n : nf) * R * (int64_t)sizeof(float);
+  const uintptr_t i0 = (uintptr_t)in, o0 = (uintptr_t)out;
+  if (i0 < o0 + (uintptr_t)out_bytes && o0 < i0 + (uintptr_t)in_bytes)
+    return fail(MBC_BAD_ARG, "mbc_point_apply_noalloc: in and out overlap (they must be distinct buffers)");
+  // an error left pending by earlier, unrelated work is reported as such and
+  // left in place, so that the launch check below sees only this call's own
+  const cudaError_t prior = cudaPeekAtLastError();
+  if (prior != cudaSuccess)
+    return fail(MBC_CUDA_ERROR, std::string("mbc_point_apply_noalloc: an earlier CUDA error is pending (not "
+                                            "cleared, nothing launched): ") + cudaGetErrorString(prior));
   float4 *base = nullptr;
   if (mbc_status s = scratch_for_current_device(&base)) return s;
   float4 *x4 = base, *n4 = base + round16(nf), *y4 = base + 2 * round16(nf);

@@ -990,9 +990,14 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
         gather_cols_kernel<T><<<cdiv(ns, 256), 256, 0, st>>>(n, R, Rs, d_idx, w.Rv, ws.Rv);
         launches += 2;
         MBC_CKL();
-        MBC_TRY((run_pcg<T, double, T>(*this, Rs, ws, ws.X, (const double *)lval.ptr, o.max_iters, o.tol,
-                                       o.precondition != 0, std::max(1, o.check_every), nullptr, st, d_b2s,
-                                       nullptr, 0, compact)));
+        if (precision == MBC_F64)
+          MBC_TRY((run_pcg<T, double, T>(*this, Rs, ws, ws.X, (const double *)lval.ptr, o.max_iters, o.tol,
+                                         o.precondition != 0, std::max(1, o.check_every), nullptr, st, d_b2s,
+                                         nullptr, 0, compact)));
+        else
+          MBC_TRY((run_pcg<T, float, T>(*this, Rs, ws, ws.X, (const float *)lval.ptr, o.max_iters, o.tol,
+                                        o.precondition != 0, std::max(1, o.check_every), nullptr, st, d_b2s,
+                                        nullptr, 0, compact)));
         std::vector<int32_t> it2(Rs);
         MBC_CK(cudaMemcpyAsync(it2.data(), ws.sc.iters, sizeof(int32_t) * Rs, cudaMemcpyDeviceToHost, st));
         scatter_cols_kernel<T><<<cdiv(ns, 256), 256, 0, st>>>(n, R, Rs, d_idx, ws.X, w.X);
@@ -1229,8 +1234,8 @@ mbc_status Solver::solve(int R, const void *rhs, int32_t rhs_dt, void *X, int32_
       mbc_solve_stats s1{};
       int32_t it1 = 0;
       mbc_solve_options o1 = o;
-      if (precision == MBC_F64 || o.max_refine <= 0)
-        rs = precision == MBC_F64
+      if (precision == MBC_F64 || o.fp64_recursion || o.max_refine <= 0)
+        rs = (precision == MBC_F64 || o.fp64_recursion)
                  ? solve_plain<double>(1, cin, rhs_dt, cout, x_dt, X0 ? cx0 : nullptr, adjoint, o1, &s1, &it1, st)
                  : solve_plain<float>(1, cin, rhs_dt, cout, x_dt, X0 ? cx0 : nullptr, adjoint, o1, &s1, &it1, st);
       else
@@ -1250,7 +1255,8 @@ mbc_status Solver::solve(int R, const void *rhs, int32_t rhs_dt, void *X, int32_
     agg.status_per_worst = worst;
     MBC_CK(cudaStreamSynchronize(st));
     if (stats) *stats = agg;
-  } else if (precision == MBC_F64) {
+  } else if (precision == MBC_F64 || o.fp64_recursion) {
+    // MBC_F32 with fp64_recursion: FP64 PCG preconditioned by the FP32 factor
     rs = solve_plain<double>(R, rhs, rhs_dt, X, x_dt, X0, adjoint, o, stats, iters_host, st);
   } else if (o.max_refine <= 0) {
     rs = solve_plain<float>(R, rhs, rhs_dt, X, x_dt, X0, adjoint, o, stats, iters_host, st);
@@ -1428,6 +1434,7 @@ extern "C" void mbc_solve_default_options(mbc_solve_options *o)
   o->profile = 0;
   o->graph = 0;
   o->compact = 0;
+  o->fp64_recursion = 0;
 }
 
 static mbc_status check_solve_args(mbc_solver *s, int32_t R, const void *in, int32_t in_dt, void *X,

@@ -146,7 +146,7 @@ def _setup_context(ctx, inputs, output):
 
 
 def _backward(ctx, grad):
-    """grad_M = -M (W + W^T) + F LV, grad_F = M VpL (core/mfs_torch_py/ops.py:51-67)."""
+    """grad_M = -M (W + W^T) + F LV, grad_F = M VpL (core/mfs_torch_py/ops.py:42-58)."""
     grad_M, grad_F = None, None
     if ctx.needs_input_grad[0] or ctx.needs_input_grad[1]:
         M, F, Vs_s, A = ctx.saved_tensors

@@ -192,6 +192,10 @@ typedef struct {
                             least 8 have stopped), continue with those columns alone, so the
                             matvecs carry only them (FP64 and plain FP32 solves, and the
                             FP64 polish of MBC_F32 solves) */
+  int32_t fp64_recursion; /* MBC_F32 solvers: run the whole PCG in FP64 (vectors, dot products,
+                            scalars and the FP64 matvec chosen by mbc_solver_set_fp64_matvec),
+                            keeping only the factor and its application in FP32; max_refine and
+                            inner_tol are then unused.  Ignored by MBC_F64 solvers. */
 } mbc_solve_options;
 
 typedef struct {
@@ -322,7 +326,10 @@ mbc_status mbc_mesh_assemble(int32_t n_vert, const float *V, int32_t n_faces, co
  * address up (with that device current); make that first call before any
  * stream capture.  All calls share the array and each rewrites the parts it
  * reads, so calls whose kernels overlap on the GPU (different streams, or
- * several host threads) race: serialise them. */
+ * several host threads) race: serialise them.  `in` and `out` must not
+ * overlap (MBC_BAD_ARG).  A CUDA error already pending when the call starts is
+ * returned as MBC_CUDA_ERROR and left pending.  The array's address is cached
+ * per device: after cudaDeviceReset, do not call this again in the process. */
 mbc_status mbc_point_apply_noalloc(int32_t transpose, int32_t nf, int32_t n, const float *x,
                                    const float *nx, const float *y, double coef, int32_t R,
                                    const float *in, float *out, mbc_stream stream);

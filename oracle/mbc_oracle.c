@@ -630,6 +630,98 @@ int orc_pcg(int nf, int n, const double *M, const double *x, const double *nx,
 }
 
 /*
+ * orc_pcg on R forward columns at once: the same per-column recurrence
+ * (kl_chol.cu:891-1088 run once per column, mfs_torch_ops.cu:162-171), with
+ * the K / K^T passes shared by the columns that still iterate so that each
+ * kernel entry is evaluated once per pass for all of them.  Every column's
+ * arithmetic is that of orc_pcg alone: orc_apply_K / orc_apply_KT sum each
+ * (row, column) over the same index order for any R, and the dot products
+ * and preconditioner run on per-column vectors.  A column stops exactly
+ * where orc_pcg would; its x, iterations and relres are those orc_pcg
+ * returns.  F: nf x R row-major (original row order); xout: n x R row-major
+ * in the NEW order; iters[R], relres[R].  Returns 0, or -1 on allocation
+ * failure.
+ */
+int orc_pcg_many(int nf, int n, const double *M, const double *x, const double *nx,
+                 const double *y, double coef, const int32_t *perm_inv, const int32_t *lptr,
+                 const int32_t *lind, const double *lval, int R, const double *F, int maxits,
+                 double tol, double *xout, int32_t *iters, double *relres)
+{
+  const size_t nn = (size_t)n, nR = (size_t)n * R;
+  double *r = (double *)malloc(sizeof(double) * nR);   /* per column, contiguous */
+  double *p = (double *)malloc(sizeof(double) * nR);
+  double *z = (double *)malloc(sizeof(double) * nR);
+  double *xc = (double *)malloc(sizeof(double) * nR);
+  double *tmp = (double *)malloc(sizeof(double) * nn);
+  double *po = (double *)malloc(sizeof(double) * nR);  /* n x A row-major, original order */
+  double *to = (double *)malloc(sizeof(double) * nR);
+  double *w = (double *)malloc(sizeof(double) * (size_t)nf * R);
+  double *col = (double *)malloc(sizeof(double) * nn);     /* t of one column */
+  double *thr = (double *)malloc(sizeof(double) * R), *rhs2 = (double *)malloc(sizeof(double) * R);
+  double *absnew = (double *)malloc(sizeof(double) * R), *resd2 = (double *)malloc(sizeof(double) * R);
+  int *act = (int *)malloc(sizeof(int) * R);
+  int c, k, A, i;
+  if (!r || !p || !z || !xc || !tmp || !po || !to || !w || !col || !thr || !rhs2 || !absnew || !resd2 || !act) {
+    free(r); free(p); free(z); free(xc); free(tmp); free(po); free(to); free(w); free(col);
+    free(thr); free(rhs2); free(absnew); free(resd2); free(act);
+    return -1;
+  }
+  /* b = K_p^T f per column (one R-column pass: same sums as R = 1) */
+  orc_apply_KT(nf, n, M, x, nx, y, coef, R, F, to);
+  A = 0;
+  for (c = 0; c < R; ++c) {
+    double *rc = r + (size_t)c * nn;
+    for (k = 0; k < n; ++k) rc[k] = to[(size_t)perm_inv[k] * R + c];
+    for (k = 0; k < n; ++k) xc[(size_t)c * nn + k] = 0.0;
+    rhs2[c] = dotv(n, rc, rc);
+    iters[c] = 0;
+    resd2[c] = 0.0;
+    relres[c] = 0.0;
+    if (rhs2[c] < 1e-16) continue;
+    thr[c] = tol * tol * rhs2[c];
+    orc_precond(n, lptr, lind, lval, rc, tmp, p + (size_t)c * nn);
+    absnew[c] = dotv(n, rc, p + (size_t)c * nn);
+    act[A++] = c;
+  }
+  while (A > 0) {
+    int A2 = 0;
+    for (i = 0; i < A; ++i) {
+      const double *pc = p + (size_t)act[i] * nn;
+      for (k = 0; k < n; ++k) po[(size_t)perm_inv[k] * A + i] = pc[k];
+    }
+    orc_apply_K(nf, n, M, x, nx, y, coef, A, po, w);
+    orc_apply_KT(nf, n, M, x, nx, y, coef, A, w, to);
+    for (i = 0; i < A; ++i) {
+      c = act[i];
+      double *rc = r + (size_t)c * nn, *pc = p + (size_t)c * nn, *zc = z + (size_t)c * nn;
+      double *xcc = xc + (size_t)c * nn, *t = col;
+      double alpha, beta, absold;
+      ++iters[c];
+      for (k = 0; k < n; ++k) t[k] = to[(size_t)perm_inv[k] * A + i];
+      alpha = absnew[c] / dotv(n, pc, t);
+      for (k = 0; k < n; ++k) xcc[k] += alpha * pc[k];
+      for (k = 0; k < n; ++k) rc[k] -= alpha * t[k];
+      resd2[c] = dotv(n, rc, rc);
+      if (resd2[c] < thr[c] || iters[c] >= maxits) continue;
+      orc_precond(n, lptr, lind, lval, rc, tmp, zc);
+      absold = absnew[c];
+      absnew[c] = dotv(n, rc, zc);
+      beta = absnew[c] / absold;
+      for (k = 0; k < n; ++k) pc[k] = beta * pc[k] + zc[k];
+      act[A2++] = c;
+    }
+    A = A2;
+  }
+  for (c = 0; c < R; ++c) {
+    if (rhs2[c] >= 1e-16) relres[c] = sqrt(resd2[c] / rhs2[c]);
+    for (k = 0; k < n; ++k) xout[(size_t)k * R + c] = xc[(size_t)c * nn + k];
+  }
+  free(r); free(p); free(z); free(xc); free(tmp); free(po); free(to); free(w); free(col);
+  free(thr); free(rhs2); free(absnew); free(resd2); free(act);
+  return 0;
+}
+
+/*
  * Added-mass tensor of a solved scene (the parity observable downstream of
  * the solve): core/KTAB_Mfs_spclf1d.py:123-128 with utils/torch_utils.py
  * compute_single_layer (:254-276) and compute_quadrature (:336-347).

@@ -69,6 +69,9 @@ def lib():
         L.orc_pcg.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, C.c_double, _i32p, _i32p, _i32p,
                               _f64p, C.c_int, vp, vp, C.c_int, C.c_int, C.c_double, _f64p,
                               C.POINTER(C.c_double)]
+        L.orc_pcg_many.restype = C.c_int
+        L.orc_pcg_many.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, C.c_double, _i32p, _i32p, _i32p,
+                                   _f64p, C.c_int, _f64p, C.c_int, C.c_double, _f64p, _i32p, _f64p]
         L.orc_num_threads.restype = C.c_int
         _lib = L
     return _lib
@@ -267,6 +270,21 @@ def pcg(op: Op, pl: dict, lval, f=None, b=None, maxits=1000, tol=1e-8, precond=T
                        1 if b is not None else 0, _vp(fa), _vp(ba), 1 if precond else 0,
                        int(maxits), float(tol), x, C.byref(rr))
     return x, it, rr.value
+
+
+def pcg_many(op: Op, pl: dict, lval, F, maxits=1000, tol=1e-8):
+    """orc_pcg on every column of F (nf x R) with shared K / K^T passes:
+    per column the same x, iterations and relres as pcg(f=F[:, c]).
+    Returns (X new order n x R, iters int32[R], relres[R])."""
+    F = np.ascontiguousarray(np.atleast_2d(np.asarray(F, np.float64).T).T)
+    R = F.shape[1]
+    X = np.empty((op.n, R))
+    its = np.empty(R, np.int32)
+    rel = np.empty(R)
+    if lib().orc_pcg_many(*op.args(), pl["Pinv"], pl["lptr"], np.ascontiguousarray(pl["lind"], np.int32),
+                          lval, R, F.reshape(-1), int(maxits), float(tol), X.reshape(-1), its, rel) != 0:
+        raise MemoryError("orc_pcg_many")
+    return X, its, rel
 
 
 def solve(op: Op, pl: dict, lval, F, maxits=1000, tol=1e-8):

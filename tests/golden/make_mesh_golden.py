@@ -22,10 +22,14 @@ sys.path[:0] = [ROOT]
 
 from fastmbcui_b200 import scenes as S  # noqa: E402
 
-REF = os.environ.get("MBC_REFERENCE", "/root/reference")
+# the reference tree (the directory holding utils/torch_utils.py): required,
+# from the environment, with no default location
+REF = os.environ.get("MBC_REFERENCE", "")
 
 
 def _reference_utils():
+    if not REF or not os.path.isfile(os.path.join(REF, "utils", "torch_utils.py")):
+        raise SystemExit("set MBC_REFERENCE to the reference tree (the directory with utils/torch_utils.py)")
     spec = importlib.util.spec_from_file_location("ref_torch_utils", os.path.join(REF, "utils", "torch_utils.py"))
     mod = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mod)

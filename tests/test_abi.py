@@ -60,8 +60,8 @@ def test_context_lifecycle_without_gpu():
 
 def test_default_options_set_every_field():
     """mbc_solve_default_options writes every field of mbc_solve_options, so a
-    C caller's struct on the stack holds no garbage afterwards (compact, the
-    newest field, included)."""
+    C caller's struct on the stack holds no garbage afterwards (fp64_recursion,
+    the newest field, included)."""
     import ctypes as C
 
     from fastmbcui_b200 import _lib, load
@@ -70,7 +70,8 @@ def test_default_options_set_every_field():
     C.memset(C.byref(o), 0xFF, C.sizeof(o))
     load().mbc_solve_default_options(C.byref(o))
     want = {"max_iters": 1000, "tol": 1e-8, "schedule": 0, "precondition": 1, "max_refine": 64,
-            "inner_tol": 1e-2, "check_every": 8, "true_residual": 0, "profile": 0, "graph": 0, "compact": 0}
+            "inner_tol": 1e-2, "check_every": 8, "true_residual": 0, "profile": 0, "graph": 0, "compact": 0,
+            "fp64_recursion": 0}
     assert {k for k, _ in _lib.SolveOptions._fields_} == set(want)
     for k, v in want.items():
         assert getattr(o, k) == v, k

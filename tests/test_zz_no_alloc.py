@@ -1,9 +1,11 @@
 """mbc_point_apply_noalloc: the point-kernel matvec with a static workspace.
 
-Its output is checked against the solver's own operator applications
-(mbc_apply_K / mbc_apply_KT) on the same points, within the FP32 matvec
-tolerance of the other parity tests (2e-5, norm-wise relative), over calls in
-a row that reuse the shared static array with different sizes and directions.
+Its output is checked against the FP64 oracle's K / K^T (oracle.Op, the CPU
+restatement of the point kernel) and against the library's allocating entry
+points (the solver's mbc_apply_K / mbc_apply_KT) on the same points, within
+the FP32 matvec tolerance of the other parity tests (2e-5, norm-wise
+relative), over calls in a row that reuse the shared static array with
+different sizes and directions.
 """
 import ctypes as C
 
@@ -11,6 +13,7 @@ import numpy as np
 import pytest
 
 import fastmbcui_b200 as F
+import oracle as O
 from fastmbcui_b200 import _lib
 from fastmbcui_b200 import scenes as S
 
@@ -43,15 +46,20 @@ class Scene:
         self.x, self.nx, self.y = _dev(sc.x), _dev(sc.nx), _dev(sc.y)
         plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
         self.solver = F.Solver(plan, x=self.x, nx=self.nx, y=self.y, coef=sc.coef, precision=F.MBC_F32)
+        self.op = O.Op.from_scene(sc)
 
     def check(self, transpose, R, seed):
         rng = np.random.default_rng(seed)
-        V = _dev(rng.standard_normal((self.sc.nf if transpose else self.sc.n, R)))
+        Vh = rng.standard_normal((self.sc.nf if transpose else self.sc.n, R)).astype(np.float32)
+        V = _dev(Vh)
         got = noalloc(transpose, self.x, self.nx, self.y, self.sc.coef, V)
-        want = self.solver.apply_KT(V) if transpose else self.solver.apply_K(V)
+        lib = self.solver.apply_KT(V) if transpose else self.solver.apply_K(V)
         torch.cuda.synchronize()
-        err = rel(got.double().cpu().numpy(), want.double().cpu().numpy())
+        got = got.double().cpu().numpy()
+        oracle = self.op.KT(Vh) if transpose else self.op.K(Vh)
+        err = rel(got, oracle)
         assert err < TOL, (transpose, R, err)
+        assert rel(got, lib.double().cpu().numpy()) < TOL, (transpose, R)
 
 
 @pytest.mark.gpu
@@ -84,6 +92,17 @@ def test_noalloc_largest_accepted_size():
     k = (d * nx[rows, None, :].astype(np.float64)).sum(-1) / (r2 * np.sqrt(r2))
     want = coef * k @ V.double().cpu().numpy()
     assert rel(got[rows], want) < TOL
+
+
+def test_noalloc_refuses_overlapping_buffers():
+    L = F.load()
+    p = C.c_void_p(4096)
+    # out starts inside in's 10 x 2 floats (80 bytes): refused before any launch
+    s = L.mbc_point_apply_noalloc(0, 10, 10, p, p, p, 1.0, 2, C.c_void_p(4096), C.c_void_p(4096 + 40), None)
+    assert s == _lib.MBC_BAD_ARG
+    assert b"overlap" in L.mbc_last_error()
+    s = L.mbc_point_apply_noalloc(1, 10, 10, p, p, p, 1.0, 2, C.c_void_p(4096), C.c_void_p(4096), None)
+    assert s == _lib.MBC_BAD_ARG
 
 
 def test_noalloc_refuses_sizes_beyond_the_static_scratch():
