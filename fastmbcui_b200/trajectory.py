@@ -1,0 +1,97 @@
+"""Solving a moving scene step after step.
+
+A rigid-body simulation calls the MFS solve once per time step
+(core/KTAB_Mfs_spclf1d.py:117, one MinvF_float_fastGrad call per
+compute_kirchhoff_tensor) on bodies that moved a little since the last step.
+``TrajectorySolver`` is that call for point-kernel scenes: every step builds a
+new supernodal factor on the current geometry, solves all rigid-mode columns
+in one batched PCG to the FP64 tolerance, and starts from the strengths of the
+previous steps instead of x0 = 0 (the reference always starts from zero,
+src/kl_chol.cu:930-940).
+
+Precision modes (``mode``):
+  "mixed"  the factor and its application in FP32 (supernodes whose FP32
+           Cholesky cancels are refactored in FP64); the PCG recursion,
+           dot products and scalars in FP64; the matvecs FP64-accurate
+           (``fp64_matvec="int8"``: exact digit slices on the INT8 tensor
+           cores, or "simt": FP64 CUDA cores).
+  "fp64"   the plain method: FP64 factor and FP64 PCG.
+  "fp32-replace"  FP32 recursion (tensor-core 3xTF32 matvec) with FP64
+           residual replacement and an FP64 polish of stagnating columns.
+
+Warm starts (``warm``): "extrapolate" (quadratic extrapolation of the last
+three steps' strengths, linear with two, the previous with one), "previous",
+"cold" (x0 = 0), or a callable ``warm(history) -> X0 or None``.
+Every column is still decided on its own FP64 residual, whatever the start.
+"""
+from __future__ import annotations
+
+from . import MBC_F32, MBC_F64, Solver
+
+MODES = ("mixed", "fp64", "fp32-replace")
+
+
+def extrapolate(hist):
+    """x0 from the strengths of the previous steps (newest last)."""
+    if not hist:
+        return None
+    if len(hist) >= 3:
+        return 3.0 * hist[-1] - 3.0 * hist[-2] + hist[-3]
+    if len(hist) == 2:
+        return 2.0 * hist[-1] - hist[-2]
+    return hist[-1]
+
+
+class TrajectorySolver:
+    def __init__(self, coef: float, *, mode: str = "mixed", fp64_matvec: str = "int8",
+                 warm="extrapolate", tol: float = 1e-8, max_iters: int = 3000, check_every: int = 8,
+                 compact: bool = False, matvec: int = 0):
+        if mode not in MODES:
+            raise ValueError(f"mode must be one of {MODES}")
+        self.coef, self.mode, self.fp64_matvec = float(coef), mode, fp64_matvec
+        self.warm, self.tol, self.max_iters = warm, float(tol), int(max_iters)
+        self.check_every, self.compact, self.matvec = int(check_every), bool(compact), int(matvec)
+        self.history = []
+
+    def start(self):
+        """The warm start of the next step (None: x0 = 0)."""
+        if callable(self.warm):
+            return self.warm(self.history)
+        if self.warm == "cold" or not self.history:
+            return None
+        if self.warm == "previous":
+            return self.history[-1]
+        if self.warm == "extrapolate":
+            return extrapolate(self.history)
+        raise ValueError(f"unknown warm start {self.warm!r}")
+
+    def solver(self, plan, x, nx, y):
+        """A factored solver of this mode for one step's geometry."""
+        if self.mode == "fp64":
+            s = Solver(plan, x=x, nx=nx, y=y, coef=self.coef, precision=MBC_F64)
+        else:
+            s = Solver(plan, x=x, nx=nx, y=y, coef=self.coef, precision=MBC_F32)
+            s.set_matvec(self.matvec)
+        return s.set_fp64_matvec(self.fp64_matvec).factor()
+
+    def step(self, plan, x, nx, y, F, *, X0=None, profile: int = 0, keep: bool = True):
+        """Factor on this step's geometry and solve F (nf x R); returns
+        (X (n x R, FP64 except in "fp32-replace" mode), stats).  The
+        result joins the history the next warm start is formed from unless
+        keep=False; X0 overrides the warm start."""
+        import torch
+
+        if X0 is None:
+            X0 = self.start()
+        s = self.solver(plan, x, nx, y)
+        opts = dict(X0=X0, profile=profile, tol=self.tol, max_iters=self.max_iters,
+                    check_every=self.check_every)
+        if self.mode == "fp32-replace":
+            X, st = s.solve(F, out_dtype=torch.float32, max_refine=64, inner_tol=1e-2,
+                            compact=int(self.compact), **opts)
+        else:
+            X, st = s.solve(F, out_dtype=torch.float64, compact=int(self.compact),
+                            fp64_recursion=1 if self.mode == "mixed" else 0, **opts)
+        if keep:
+            self.history = (self.history + [X])[-3:]
+        return X, st

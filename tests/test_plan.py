@@ -109,3 +109,21 @@ def test_boxes_above_floor_order_matches_reference():
     ptr, ind = O.pattern(sc.y, P, s, sc.rho)
     ptr2, ind2 = O.ref_pattern(sc.y, Pr, sr, sc.rho)
     assert np.array_equal(ptr, ptr2) and np.array_equal(ind, ind2)
+
+
+@pytest.mark.parametrize("k", [0, 3])
+def test_trajectory32_plan_matches_oracle_and_reference(k):
+    """The benchmark's scene (32 ellipsoids x 2000 points on the seed-4
+    trajectory, poses 0 and 3): the product's whole plan equals the
+    oracle's, and the oracle's ordering and pattern equal the reference's own
+    maxmin.h / nanoflann code (oracle/_ref) when it is built."""
+    base, q, _ = S.trajectory_scene(32, 2000, seed=4, steps=500)
+    sc = S.moved(base, q[k])
+    assert_same(sc.y, rho=sc.rho, lam=sc.lam, max_super=sc.max_super)
+    if O.ref_available():
+        P, s = O.order(sc.y)
+        Pr, sr = O.ref_order(sc.y)
+        assert np.array_equal(P, Pr) and np.array_equal(s, sr)
+        ptr, ind = O.pattern(sc.y, P, s, sc.rho)
+        ptr2, ind2 = O.ref_pattern(sc.y, Pr, sr, sc.rho)
+        assert np.array_equal(ptr, ptr2) and np.array_equal(ind, ind2)
