@@ -32,6 +32,12 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+T_START = time.perf_counter()
+
+
+def _left(args) -> float:
+    """Seconds of the run's wall-clock budget (--budget-s) still unspent."""
+    return args.budget_s - (time.perf_counter() - T_START)
 
 MATVEC = {"auto": 0, "simt": 1, "tensor": 2}
 
@@ -53,6 +59,8 @@ WORKLOADS = {
 def _dtype(args, fp64_only=False):
     """The arithmetic the timed path computes in."""
     f64 = "f64 (int8 digit slices, exact int32 sums)" if args.fp64_matvec == "int8" else "f64"
+    if args.solver == "mixed64":
+        return f"{f64}; f32 factor"
     return f64 if fp64_only else f"f32+{f64}"
 
 
@@ -176,226 +184,321 @@ def _max_over_ranks(dist, v: float) -> float:
 
 
 def run_trajectory(args):
-    """The 32-ellipsoid trajectory: one step = the bodies move, a new factor,
-    and the mixed batched PCG of all 192 columns warm-started from the
-    previous step's strengths (the plan of each step is host work, reported as
-    its own column)."""
+    """The 32-ellipsoid trajectory.  One step = the bodies move, a new host
+    plan, a new supernodal factor, and one batched PCG of all 192 rigid-mode
+    columns to the FP64 tolerance, warm-started from the previous steps
+    (fastmbcui_b200.trajectory.TrajectorySolver, the call a simulation makes
+    once per time step).  Inputs are resident in HBM in the timed steps; the
+    host plan is reported as its own column.  After the timed steps: the same
+    steps end to end from host buffers, the plain FP64 method on a sample of
+    columns, an ablation of the speed-up, and the CPU oracle."""
     import torch
 
     import fastmbcui_b200 as F
     from fastmbcui_b200 import scenes as S
+    from fastmbcui_b200.trajectory import TrajectorySolver
 
     dist, rank, world, local = _dist()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     base, q, _ = S.trajectory_scene(32, 2000, seed=4 + rank, steps=500)
     nsteps = args.warmup + args.steps
+    n_e2e = max(1, args.e2e_steps)
     t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
-    scenes = [S.moved(base, q[k]) for k in range(nsteps + 1)]
+    scenes = [S.moved(base, q[k]) for k in range(nsteps + n_e2e)]
     # the host plan of each step; with --plan-every K (an opt-in mode that is
     # not the plain method) the ordering, pattern and supernodes of a step are
     # reused for the next K - 1 steps and only the factor is rebuilt, on the
     # current geometry
     t0 = time.perf_counter()
     plans = []
-    for k, sc in enumerate(scenes):
+    for k, sc in enumerate(scenes[:nsteps]):
         if k % max(1, args.plan_every) == 0:
             plans.append(F.Plan(sc.y, sc.rho, sc.lam, sc.max_super))
         else:
             plans.append(plans[-1])
-    t_plan = (time.perf_counter() - t0) / len(scenes)
-    coords = [(t(sc.x), t(sc.nx), t(sc.y)) for sc in scenes]  # inputs resident in HBM
-    Fm = [t(sc.rhs()) for sc in scenes]
+    t_plan = (time.perf_counter() - t0) / nsteps
+    coords = [(t(sc.x), t(sc.nx), t(sc.y)) for sc in scenes[:nsteps]]  # inputs resident in HBM
+    Fm = [t(sc.rhs()) for sc in scenes[:nsteps]]
     R = Fm[0].shape[1]
-    opts = dict(tol=1e-8, max_iters=args.max_iters, max_refine=64, inner_tol=1e-2, check_every=8,
-                compact=int(args.compact))
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
-    # learned warm start: the trained network and the bodies' isolated
-    # solutions (a per-shape cache computed once, outside the timed steps)
-    ws = None
-    if args.warm == "learned":
-        from fastmbcui_b200 import warmstart as W
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
 
-        ws = W.WarmStart.load(args.warm_model)
-        U = W.isolated_basis(base)
-        sb = torch.as_tensor(base.src_body, dtype=torch.int32, device=dev)
-
-    def start(k, hist):
-        """x0 of step k from the strengths of the previous steps (newest last)."""
-        if not hist or args.warm == "cold":
-            return None
-        if args.warm == "previous":
-            return hist[-1]
-        if args.warm == "learned":
-            pairs = W.neighbour_pairs(scenes[k].centers)
-            f = W.pair_features(pairs, q[k - 1], q[k], base.centers, base.meta["axes"], base.meta["rot"])
-            return ws.apply(hist[-1].float(), U, sb, base.n_bodies, pairs, f).to(hist[-1].dtype)
-        # polynomial extrapolation along the smooth trajectory (quadratic once
-        # three steps are known): ~40 % fewer FP64 iterations than x(t-1)
-        if len(hist) >= 3:
-            return 3.0 * hist[-1] - 3.0 * hist[-2] + hist[-3]
-        if len(hist) == 2:
-            return 2.0 * hist[-1] - hist[-2]
-        return hist[-1]
-
-    out_dt = torch.float64 if args.solver in ("fp64", "mixed64") else torch.float32
-
-    def solve_scene(plan, x, nx, y, Fk, X0, profile=0):
-        """One step's factor and solve through the selected path."""
-        if args.solver == "mixed64":
-            # FP32 factor (FP64 retry of cancelling supernodes) preconditioning
-            # an FP64 PCG whose matvecs follow --fp64-matvec
-            s = F.Solver(plan, x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F32)
-            s.set_fp64_matvec(args.fp64_matvec).factor()
-            return s.solve(Fk, X0=X0, out_dtype=torch.float64, profile=profile, tol=1e-8,
-                           max_iters=args.max_iters, check_every=8, compact=int(args.compact), fp64_recursion=1)
-        if args.solver == "fp64":
-            # FP64 PCG with the FP64 factor; with --fp64-matvec int8 its
-            # matvecs run on the INT8 tensor cores
-            s64 = F.Solver(plan, x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64)
-            s64.set_fp64_matvec(args.fp64_matvec).factor()
-            return s64.solve(Fk, X0=X0, out_dtype=torch.float64, profile=profile, tol=1e-8,
-                             max_iters=args.max_iters, check_every=8, compact=int(args.compact))
-        s = F.Solver(plan, x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F32)
-        s.set_matvec(MATVEC[args.matvec]).set_fp64_matvec(args.fp64_matvec).factor()
-        if args.solver == "flexible":
-            # FP64 flexible CG around the FP32 PCG; the FP64 solver only applies K
-            from fastmbcui_b200.flexible import solve_flexible
-
-            s64 = F.Solver(plan, x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64)
-            s64.set_fp64_matvec(args.fp64_matvec)
-            X, info = solve_flexible(s64, s, Fk, tol=1e-8, inner_iters=args.inner_iters, X0=X0,
-                                     profile=bool(profile))
-            st = {"iters_max": info["fp32_inner_iterations"], "iters_total": info["fp32_inner_iterations"] * R,
-                  "refinements": info["fp64_applies"], "n_polished": 0, "true_relres_max": info["relres_max"],
-                  "n_converged": info["converged"], "kernel_launches": info["kernel_launches"],
-                  "n_matvec": info["n_matvec64"] + info["n_matvec32"],
-                  "t_matvec_ms": info["t_matvec64_ms"] + info["t_matvec32_ms"],
-                  "n_matvec64": info["n_matvec64"], "t_matvec64_ms": info["t_matvec64_ms"]}
-            return X.float(), st
-        return s.solve(Fk, X0=X0, out_dtype=torch.float32, profile=profile, **opts)
-
-    def step(k, hist, profile=0):
-        x, nx, y = coords[k]
-        return solve_scene(plans[k], x, nx, y, Fm[k], start(k, hist), profile)
-
-    hist = []
+    warm = args.warm
+    if warm == "learned":
+        warm = _learned_start(args, base, q, scenes, dev)
+    mode = {"mixed64": "mixed", "mixed": "fp32-replace"}.get(args.solver, args.solver)
+    ts = TrajectorySolver(base.coef, mode=mode, fp64_matvec=args.fp64_matvec, warm=warm,
+                          max_iters=args.max_iters, compact=args.compact, matvec=MATVEC[args.matvec])
     cold = None
     for k in range(args.warmup):
-        X, st = step(k, hist)
-        hist = (hist + [X])[-3:]
+        if callable(warm):
+            warm.k = k
+        _, st = ts.step(plans[k], *coords[k], Fm[k])
         if k == 0:
             cold = st
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     times, stats = [], []
+    # the wall-clock budget: the timed steps stop early (steps_run < steps)
+    # when one more would leave less than the reserve the later legs need;
+    # rank 0 decides for every rank
     with ClockSampler(local) as clk:
         for k in range(args.warmup, nsteps):
+            if callable(warm):
+                warm.k = k
             flush.fill_(float(k))
             if dist:
                 dist.barrier()
             torch.cuda.synchronize()
+            t_wall = time.perf_counter()
             ev0.record()
-            X, st = step(k, hist, profile=1)
+            X, st = ts.step(plans[k], *coords[k], Fm[k], profile=1)
             ev1.record()
             torch.cuda.synchronize()
-            hist = (hist + [X])[-3:]
             times.append(ev0.elapsed_time(ev1))
             stats.append(st)
+            stop = _left(args) - 1.5 * (time.perf_counter() - t_wall) < args.reserve_s
+            if dist:
+                flag = torch.tensor([1.0 if stop else 0.0], device=dev)
+                dist.broadcast(flag, 0)
+                stop = bool(flag.item())
+            if stop:
+                break
     ms_step = _max_over_ranks(dist, float(np.mean(times)))
     value = world * 1000.0 / ms_step
 
-    # end to end through the public API: host coordinates and the previous
-    # steps' host strengths in, host strengths out, the host plan included
-    k = nsteps
-    sc = scenes[k]
-    pin = lambda a, dt=np.float32: torch.from_numpy(np.ascontiguousarray(a, dt)).pin_memory()
-    hx, hnx, hy, hF = pin(sc.x), pin(sc.nx), pin(sc.y), pin(sc.rhs())
-    hH = [pin(h.cpu().numpy(), h.cpu().numpy().dtype) for h in hist]
-    hX = torch.empty((sc.n, R), dtype=out_dt).pin_memory()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    dx, dnx, dy, dF = (a.to(dev, non_blocking=True) for a in (hx, hnx, hy, hF))
-    dH = [h.to(dev, non_blocking=True) for h in hH]
-    pl2 = F.Plan(sc.y.astype(np.float64), sc.rho, sc.lam, sc.max_super)
-    X2, _ = solve_scene(pl2, dx, dnx, dy, dF, start(k, dH))
-    hX.copy_(X2)
-    torch.cuda.synchronize()
-    e2e_ms = (time.perf_counter() - t0) * 1000
-    e2e = world * 1000.0 / _max_over_ranks(dist, e2e_ms)
-    h2d = sum(a.numel() * a.element_size() for a in [hx, hnx, hy, hF] + hH)
-    d2h = hX.numel() * hX.element_size()
-    del X2, pl2
-
-    # plain FP64 GPU path on the first timed step: one cold-started PCG per
-    # column, a bounded sample of columns extrapolated to all R
-    k = args.warmup
-    x, nx, y = coords[k]
-    plain = F.Solver(plans[k], x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64)
-    ncol = min(R, args.plain_cols)
-    cols = np.linspace(0, R - 1, ncol).astype(int)
-    torch.cuda.synchronize()
-    ev0.record()
-    plain.factor()
-    ev1.record()
-    torch.cuda.synchronize()
-    t_fac64 = ev0.elapsed_time(ev1)
-    ev0.record()
-    Xp, stp = plain.solve(Fm[k][:, cols].double().contiguous(), tol=1e-8, max_iters=args.max_iters,
-                          schedule=F.MBC_SCHED_PER_RHS, check_every=8)
-    ev1.record()
-    torch.cuda.synchronize()
-    t_cols = ev0.elapsed_time(ev1)
-    plain_ms = t_fac64 + t_cols * R / ncol
-    plain_sps = 1000.0 / _max_over_ranks(dist, plain_ms)
-    del plain
+    # end to end through the public API, continuing the trajectory: host
+    # coordinates and right-hand side in (pinned), the host plan, the factor
+    # and the solve (history kept on the device by the TrajectorySolver, as
+    # in a simulation loop), host strengths out
+    e2e_ms, h2d, d2h = [], 0, 0
+    for j in range(n_e2e):
+        k = nsteps + j
+        sc = scenes[k]
+        if callable(warm):
+            warm.k = k
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory()
+        hx, hnx, hy, hF = pin(sc.x), pin(sc.nx), pin(sc.y), pin(sc.rhs())
+        hX = torch.empty((sc.n, R), dtype=torch.float64).pin_memory()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dx, dnx, dy, dF = (a.to(dev, non_blocking=True) for a in (hx, hnx, hy, hF))
+        pl = F.Plan(sc.y.astype(np.float64), sc.rho, sc.lam, sc.max_super)
+        X2, _ = ts.step(pl, dx, dnx, dy, dF)
+        hX.copy_(X2)
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - t0) * 1000)
+        h2d = sum(a.numel() * a.element_size() for a in (hx, hnx, hy, hF))
+        d2h = hX.numel() * hX.element_size()
+        del X2, pl
+    e2e = world * 1000.0 / _max_over_ranks(dist, float(np.mean(e2e_ms)))
 
     st = stats[-1]
-    roofline = _matvec_roofline(st, scenes[0].nf, scenes[0].n, R, args.matvec, args.fp64_matvec)
     out = {
         "metric": METRIC, "value": round(value, 5), "unit": "solves/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": _dtype(args, args.solver == "fp64"),
+        "steps": len(times), "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": _dtype(args, args.solver in ("fp64", "mixed64")),
         "data": "synthetic (seeded trajectory)",
         "config": {"workload": "trajectory32", "desc": WORKLOADS["trajectory32"][1], "N": base.n,
                    "Nf": base.nf, "R": R, "rho": base.rho, "lambda": base.lam, "tol": 1e-8,
-                   "precision": {"flexible": "FP64 flexible CG around FP32 PCG",
-                                 "fp64": "FP64 PCG, FP64 factor",
-                                 "mixed64": "FP64 PCG, FP32 factor",
-                                 "mixed": "mixed FP32/FP64 residual replacement"}[args.solver],
-                   "schedule": "batched",
-                   "warm_start": {"learned": "previous step + MLP correction (3x256, BF16 weights)",
-                                  "extrapolate": "quadratic extrapolation of the last three steps' strengths",
-                                  "previous": "previous step's strengths", "cold": "x0 = 0"}[args.warm],
-                   "steps_run": f"{args.warmup} warm-up + {args.steps} timed",
+                   "precision": PRECISION[args.solver], "schedule": "batched",
+                   "warm_start": WARM[args.warm],
+                   "steps_requested": args.steps, "steps_run": len(times),
                    "plan_every": args.plan_every, "solver": args.solver, "fp64_matvec": args.fp64_matvec,
                    "compact": bool(args.compact) and args.solver != "flexible",
                    "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas{world}"},
         "e2e": {"value": round(e2e, 5), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h),
-                "includes": "H2D of points, rhs and the last steps' strengths; host plan; factor; solve; D2H"},
+                "d2h_bytes_per_step": int(d2h), "steps": n_e2e,
+                "includes": "H2D of coordinates and right-hand side from pinned memory; host plan; factor; "
+                            "solve (history on the device); D2H of the FP64 strengths"},
         "gpu_launches": int(np.mean([s_["kernel_launches"] for s_ in stats])),
-        "plain_fp64": {"solves_per_s": round(plain_sps, 6), "ms_per_solve": round(plain_ms, 1),
-                       "sample": f"{ncol} of {R} columns, per-RHS cold start, extrapolated",
-                       "iters_max": int(stp["iters_max"])},
-        "speedup_vs_plain_fp64": round(value / plain_sps, 2),
         "solve": {"iters_max": [int(s_["iters_max"]) for s_ in stats],
+                  "iters_total": [int(s_["iters_total"]) for s_ in stats],
                   "iters_max_cold_first_step": int(cold["iters_max"]) if cold else None,
-                  "refinements": [int(s_["refinements"]) for s_ in stats],
-                  "n_polished": [int(s_["n_polished"]) for s_ in stats],
                   "true_relres_max": max(s_["true_relres_max"] for s_ in stats),
-                  "n_converged": [int(s_["n_converged"]) for s_ in stats]},
+                  "n_converged": [int(s_["n_converged"]) for s_ in stats],
+                  "ms": [round(x, 1) for x in times]},
         "host_plan_ms": round(t_plan * 1000, 1),
-        "roofline": roofline,
+        "roofline": _matvec_roofline(st, base.nf, base.n, R, args.matvec, args.fp64_matvec),
         "clocks": clk.summary(),
     }
-    if rank == 0 and world == 1 and not args.no_cpu:
-        out["cpu_baseline"] = cpu_baseline(scenes[args.warmup], st)
+    # the plain FP64 method (the reference's algorithm in FP64: one cold PCG
+    # per column, FP64 factor, FP64 CUDA-core matvec) on the trajectory's first
+    # pose, the pose of the CPU oracle's iteration fixture
+    if _left(args) > args.reserve_s * 0.5:
+        out["plain_fp64"] = _plain_leg(args, F, plans[0] if args.plan_every == 1 else None, scenes[0], t, R)
+        if out["plain_fp64"].get("solves_per_s"):
+            out["speedup_vs_plain_fp64"] = round(value / out["plain_fp64"]["solves_per_s"], 2)
+    if args.ablation and _left(args) > args.reserve_s * 0.35:
+        out["ablation"] = _ablation(args, F, TrajectorySolver, base, plans, coords, Fm, R,
+                                    out.get("plain_fp64"), value, ts)
+    if rank == 0 and world == 1 and not args.no_cpu and _left(args) > 60:
+        out["cpu_baseline"] = cpu_baseline(scenes[0], _oracle_iters(st, R))
+    out["wall_s"] = round(time.perf_counter() - T_START, 1)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+PRECISION = {"flexible": "FP64 flexible CG around FP32 PCG",
+             "fp64": "the plain method: FP64 factor, FP64 PCG",
+             "mixed64": "FP32 factor and preconditioner (FP64 retry of cancelling supernodes); FP64 PCG "
+                        "vectors, dots and scalars; FP64-accurate matvec",
+             "mixed": "FP32 PCG recursion with FP64 residual replacement and FP64 polish"}
+WARM = {"learned": "quadratic extrapolation + MLP correction (3x256, BF16 weights)",
+        "extrapolate": "quadratic extrapolation of the last three steps' strengths",
+        "previous": "previous step's strengths", "cold": "x0 = 0"}
+
+
+def _plain_leg(args, F, plan, sc, t, R):
+    """The plain FP64 method on one pose: FP64 factor, then one cold FP64 PCG
+    per column (FP64 CUDA-core matvec), the oracle fixture's columns first,
+    for at most --plain-s seconds (at least two columns); the mean time per
+    column is extrapolated to all R."""
+    import torch
+
+    if plan is None:
+        plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
+    x, nx, y = t(sc.x), t(sc.nx), t(sc.y)
+    Fd = t(sc.rhs(), torch.float64)
+    fx = _oracle_fixture()
+    order = list(fx["columns"]) if fx else []
+    order += [c for c in np.linspace(0, R - 1, 8).astype(int).tolist() if c not in order]
+    plain = F.Solver(plan, x=x, nx=nx, y=y, coef=sc.coef, precision=F.MBC_F64)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    plain.factor()
+    ev1.record()
+    torch.cuda.synchronize()
+    t_fac = ev0.elapsed_time(ev1)
+    cols, its, ms = [], [], []
+    t_leg = time.perf_counter()
+    for c in order:
+        if len(cols) >= 2 and (time.perf_counter() - t_leg > args.plain_s or _left(args) < 120):
+            break
+        ev0.record()
+        _, _, it1 = plain.solve(Fd[:, c].contiguous(), tol=1e-8, max_iters=args.max_iters, check_every=8,
+                                iters=True)
+        ev1.record()
+        torch.cuda.synchronize()
+        cols.append(int(c))
+        its.append(int(it1[0]))
+        ms.append(ev0.elapsed_time(ev1))
+    plain_ms = t_fac + float(np.mean(ms)) * R
+    rec = {"solves_per_s": round(1000.0 / plain_ms, 6), "ms_per_solve": round(plain_ms, 1),
+           "factor_ms": round(t_fac, 1), "columns": cols, "iters": its,
+           "ms_per_column": [round(v, 1) for v in ms],
+           "sample": f"{len(cols)} of {R} columns timed (per-RHS cold start), mean extrapolated to {R}",
+           "extrapolated": len(cols) < R}
+    if fx:
+        ref = dict(zip(fx["columns"], fx["iters"]))
+        rec["oracle_iters"] = [ref.get(c) for c in cols]
+    return rec
+
+
+def _ablation(args, F, TS, base, plans, coords, Fm, R, plain, value, ts_main):
+    """Where the speed-up comes from, on the first timed pose (solves/s):
+      plain     per-RHS cold FP64 PCG, FP64 CUDA-core matvec (the plain leg);
+      batched   all R columns in one cold FP64 PCG on the FP64 CUDA-core
+                matvec: 16 iterations timed, scaled to the iterations of the
+                same batched solve on the INT8 matvec (same recurrences);
+      int8      the same batched cold solve on the INT8 tensor-core matvec, timed;
+      warm      + the quadratic-extrapolation start (FP64 factor), timed;
+      mixed     + the FP32 factor (the timed steps' own mode)."""
+    import torch
+
+    k = args.warmup
+    x, nx, y = coords[k]
+    rec = {"pose": k}
+    if plain:
+        rec["plain"] = plain["solves_per_s"]
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    F64 = Fm[k].double()
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        ev0.record()
+        r = fn()
+        ev1.record()
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1), r
+
+    # batched cold FP64 on the INT8 matvec (fully timed)
+    s8 = F.Solver(plans[k], x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64).set_fp64_matvec("int8")
+    ms_f8, _ = timed(lambda: s8.factor())
+    ms8, (_, st8) = timed(lambda: s8.solve(F64, tol=1e-8, max_iters=args.max_iters, check_every=8))
+    del s8
+    it_b = int(st8["iters_max"])
+    # batched cold FP64 on the CUDA cores: a 16-iteration sample
+    s64 = F.Solver(plans[k], x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64)
+    ms_f64, _ = timed(lambda: s64.factor())
+    ms16, _ = timed(lambda: s64.solve(F64, tol=1e-30, max_iters=16, check_every=16))
+    del s64
+    rec["batched"] = round(1000.0 / (ms_f64 + ms16 / 16 * it_b), 6)
+    rec["batched_note"] = f"16 iterations timed ({ms16:.0f} ms), scaled to {it_b} iterations"
+    rec["int8"] = round(1000.0 / (ms_f8 + ms8), 6)
+    rec["int8_iters_max"] = it_b
+    # warm-started FP64 (FP64 factor) from the timed steps' own history
+    ts = TS(base.coef, mode="fp64", fp64_matvec=args.fp64_matvec, warm="extrapolate", max_iters=args.max_iters,
+            compact=args.compact)
+    ts.history = list(ts_main.history)
+    msw, (_, stw) = timed(lambda: ts.step(plans[k], x, nx, y, Fm[k], keep=False))
+    rec["warm"] = round(1000.0 / msw, 6)
+    rec["warm_iters_max"] = int(stw["iters_max"])
+    rec["mixed"] = round(value, 6)
+    rec["note"] = ("warm uses the history at the end of the timed steps on the first timed pose: it measures "
+                   "the cost of a warm step, not that pose's own iterations")
+    return rec
+
+
+def _oracle_fixture():
+    """The CPU oracle's measured cold iterations on the trajectory's first
+    pose (tests/golden/trajectory32_oracle_iters.json), or None."""
+    p = os.path.join(ROOT, "tests", "golden", "trajectory32_oracle_iters.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except OSError:
+        return None
+
+
+def _oracle_iters(st, R):
+    """Iterations per column of the plain method for the CPU baseline: the
+    oracle's own measured mean (fixture) when present."""
+    fx = _oracle_fixture()
+    if fx:
+        return {"iters_total": float(np.mean(fx["iters"])) * R,
+                "source": f"oracle PCG measured on this pose, mean over columns {fx['columns']}"}
+    return {"iters_total": st["iters_total"], "source": "this run's GPU solve"}
+
+
+def _learned_start(args, base, q, scenes, dev):
+    """The warm start of --warm learned: x(t-1) corrected by the trained
+    network in the isolated-body basis (fastmbcui_b200.warmstart)."""
+    import torch
+
+    from fastmbcui_b200 import warmstart as W
+
+    ws = W.WarmStart.load(args.warm_model)
+    U = W.isolated_basis(base)
+    sb = torch.as_tensor(base.src_body, dtype=torch.int32, device=dev)
+
+    class Learned:
+        k = 0
+
+        def __call__(self, hist):
+            if not hist:
+                return None
+            k = self.k
+            pairs = W.neighbour_pairs(scenes[k].centers)
+            f = W.pair_features(pairs, q[k - 1], q[k], base.centers, base.meta["axes"], base.meta["rot"])
+            return ws.apply(hist[-1].float(), U, sb, base.n_bodies, pairs, f).to(hist[-1].dtype)
+
+    return Learned()
 
 
 # DRAM bytes (read + write) per launch of the tensor-core matvec at N = Nf =
@@ -761,7 +864,13 @@ def run_ours(args):
 
 
 def cpu_baseline(sc, st, plan_gpu=None):
-    """The CPU oracle (FP64 C, OpenMP) on a bounded sample of the same solve."""
+    """The CPU oracle (FP64 C, OpenMP on all host threads) on a bounded
+    sample of one solve of the plain method: the plan in full, the factor of
+    every 20th supernode scaled by its share of the Gram work
+    sum_s (20 n_s + n_s (n_s + 1) / 2), and one K + K^T pass of one column
+    (every s-th row above 1e9 entries, scaled by s) times the iterations per
+    column (st["iters_total"] / R; st["source"] says where they come from)
+    times R columns."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
@@ -770,9 +879,9 @@ def cpu_baseline(sc, st, plan_gpu=None):
     pl = O.plan(sc.y, sc.rho, sc.lam, sc.max_super)
     t_plan = time.perf_counter() - t0
     op = O.Op.from_scene(sc)
-    # factor: every 50th supernode, scaled by its share of sum n_s^2
+    # factor: every 20th supernode, scaled by its share of the Gram work
     sizes = np.diff(pl["set_ptr"]).astype(np.float64)
-    sel = np.arange(0, pl["n_super"], 50)
+    sel = np.arange(0, pl["n_super"], 20)
     sub = dict(pl)
     sub["n_super"] = len(sel)
     sub_sp = np.zeros(len(sel) + 1, np.int32)
@@ -790,7 +899,10 @@ def cpu_baseline(sc, st, plan_gpu=None):
     sub["th_ptr"] = np.concatenate([[0], np.cumsum(ss * ss)]).astype(np.int64)
     t0 = time.perf_counter()
     O.factor(op, sub)
-    t_fac = (time.perf_counter() - t0) * (sizes ** 2).sum() / float((ss.astype(np.float64) ** 2).sum())
+    # per collocation row a supernode of n_s rows costs n_s kernel
+    # evaluations (~20 flops each) and n_s (n_s + 1) / 2 Gram FMAs
+    work = lambda m: (20.0 * m + m * (m + 1) / 2.0).sum()
+    t_fac = (time.perf_counter() - t0) * work(sizes) / work(ss.astype(np.float64))
     # one PCG iteration for one column: K p and K^T w; above 1e9 entries on a
     # row subset (every s-th row, both directions), scaled by s
     stride = max(1, int(np.ceil(sc.nf * float(sc.n) / 1e9)))
@@ -802,13 +914,33 @@ def cpu_baseline(sc, st, plan_gpu=None):
     sub_op.KT(w)
     t_iter = (time.perf_counter() - t0) * stride
     R = _ncols(sc)
-    iters = max(1, int(st["iters_total"] / max(1, R)))
+    iters = max(1.0, float(st["iters_total"]) / max(1, R))
     total = t_plan + t_fac + iters * R * t_iter
+    src = st.get("source", "this run's GPU solve")
     return {"value": 1.0 / total, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
-            "sample": (f"oracle plan in full ({t_plan:.2f}s), factor of every 50th supernode scaled by "
-                       f"sum n_s^2 ({t_fac:.1f}s), one K+K^T pass for one column ({t_iter:.2f}s"
+            "extrapolated": True,
+            "sample": (f"oracle plan in full ({t_plan:.2f}s), factor of every 20th supernode scaled by "
+                       f"its Gram work ({t_fac:.1f}s), one K+K^T pass for one column ({t_iter:.2f}s"
                        f"{'' if stride == 1 else f', every {stride}th row timed and scaled'}) x "
-                       f"{iters} iterations x {R} columns")}
+                       f"{iters:.0f} iterations per column ({src}) x {R} columns")}
+
+
+def cpu_full_small(O):
+    """The CPU oracle fully timed on the single-sphere configuration
+    (icosphere subdivision 4, N = Nf = 2562, R = 6, rho 3, lambda 1.5, PCG
+    to 1e-10): plan, factor and six cold PCG solves, nothing extrapolated."""
+    from fastmbcui_b200 import scenes as S
+
+    sc = S.sphere_scene()
+    t0 = time.perf_counter()
+    pl = O.plan(sc.y, sc.rho, sc.lam, sc.max_super)
+    op = O.Op.from_scene(sc)
+    _, lval, _ = O.factor(op, pl)
+    _, its = O.solve(op, pl, lval, sc.rhs(), maxits=5000, tol=1e-10)
+    sec = time.perf_counter() - t0
+    return {"workload": "sphere: icosphere subdivision 4, N=Nf=2562, R=6, PCG to 1e-10",
+            "value": round(1.0 / sec, 4), "unit": "solves/s", "seconds": round(sec, 3),
+            "iters": [int(i) for i in its], "cores": O.num_threads(), "extrapolated": False}
 
 
 def run_probe(args):
@@ -869,8 +1001,13 @@ def run_probe(args):
 
 
 def run_reference(args):
-    """The reference's CPU path on the host cores (the oracle port: the
-    reference's own host code cannot be built here beyond the ordering)."""
+    """The reference's CPU path on the host cores: its own host code does not
+    build here beyond the ordering (Eigen), so the oracle port stands in
+    (plain method, FP64, OpenMP on all host threads).  Each step is a bounded
+    sample of one solve of the workload (cpu_baseline), with the iterations
+    per column the oracle itself measured on this scene when the fixture is
+    present; the line also carries a fully timed run of the single-sphere
+    configuration."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -881,25 +1018,40 @@ def run_reference(args):
     import oracle as O
 
     O.build()
-    st = {"iters_total": args.ref_iters * _ncols(sc)}
-    vals = []
+    R = _ncols(sc)
+    fx = _oracle_fixture() if args.workload == "trajectory32" else None
+    if fx:
+        st = {"iters_total": float(np.mean(fx["iters"])) * R,
+              "source": f"oracle PCG measured on this pose, mean over columns {fx['columns']}"}
+    else:
+        st = {"iters_total": args.ref_iters * R, "source": "assumed"}
     for _ in range(max(1, args.warmup)):
         cpu_baseline(sc, st)
-    samples = []
+        if _left(args) < args.budget_s / 2:
+            break
+    vals, samples = [], []
     for _ in range(args.steps):
         b = cpu_baseline(sc, st)
         vals.append(b["value"])
         samples.append(b["sample"])
+        if _left(args) < 120:
+            break
     v = float(np.mean(vals))
-    out = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+    out = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": ws, "steps": len(vals),
            "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene)",
-           "config": {"workload": args.workload, "desc": desc, "N": sc.n, "Nf": sc.nf,
-                      "R": _ncols(sc), "iterations_assumed": args.ref_iters},
-           "impl": "reference",
+           "config": {"workload": args.workload, "desc": desc, "N": sc.n, "Nf": sc.nf, "R": R,
+                      "iterations_per_column": round(st["iters_total"] / R, 1),
+                      "iterations_source": st["source"], "steps_requested": args.steps},
+           "impl": "reference", "extrapolated": True,
            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
-                            "sample": samples[-1]},
+                            "sample": samples[-1], "extrapolated": True},
            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if fx:
+        out["oracle_fixture"] = {"columns": fx["columns"], "iters": fx["iters"],
+                                 "pcg_seconds_per_iteration": fx.get("pcg_seconds_per_iteration"),
+                                 "host_threads": fx.get("host_threads")}
+    out["full_small"] = cpu_full_small(O)
     print(json.dumps(out), flush=True)
 
 
@@ -912,11 +1064,19 @@ def main():
     ap.add_argument("--workload", default="trajectory32", choices=sorted(WORKLOADS))
     ap.add_argument("--max-iters", type=int, default=3000)
     ap.add_argument("--plain-cols", type=int, default=2)
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--plain-s", type=float, default=90.0,
+                    help="trajectory: seconds for the plain FP64 leg's per-column solves (at least two columns)")
+    ap.add_argument("--ablation", type=int, default=1, help="trajectory: 1 = time the ablation of the speed-up")
+    ap.add_argument("--e2e-steps", type=int, default=2)
     # the plain FP64 PCG's iterations per column on the 32-ellipsoid scene
     # (measured on the GPU, the same algorithm as the CPU port)
     ap.add_argument("--ref-iters", type=int, default=572)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--budget-s", type=float, default=1500.0,
+                    help="wall-clock budget of the whole run: timed steps stop early (steps_run < steps) "
+                         "so that the line is printed within it")
+    ap.add_argument("--reserve-s", type=float, default=420.0,
+                    help="seconds kept for the legs after the timed steps (e2e, plain FP64, ablation, CPU)")
     ap.add_argument("--scenes", type=int, default=8, help="uneven workload: scenes in the sample")
     ap.add_argument("--solver", default="mixed", choices=["mixed", "flexible", "fp64", "mixed64"],
                     help="trajectory and uneven: residual-replacement mixed PCG, FP64 flexible CG around the "
