@@ -26,6 +26,7 @@ struct PcgScalars {
   int32_t maxit;
   double tol2;
   double drop2;    // > 0: replacement mode, replace once |r|^2 < drop2 * rr_ref
+  int32_t stall_check;  // replacement mode: 1 = mark columns stagnant (COL_STAGNANT)
 };
 
 // Block reduction over threadIdx.y of one double per thread; thread (x, 0)
@@ -214,7 +215,7 @@ __global__ void __launch_bounds__(1024) reduce_kernel(int nblk, int R,
               sc.status[c] = COL_BREAKDOWN;
             } else if (s < sc.thr[c]) {
               sc.status[c] = COL_OK;
-            } else {
+            } else if (sc.stall_check) {
               sc.stall[c] = s > 0.25 * prev ? sc.stall[c] + 1 : 0;
               if (sc.stall[c] >= 3 && sc.status[c] == COL_ACTIVE) sc.status[c] = COL_STAGNANT;
             }
