@@ -82,6 +82,15 @@ class Plan:
         return lp, li[:self.info.factor_nnz]
 
 
+def spatial_order(pts) -> np.ndarray:
+    """Morton (Z-curve) order of points (n x 3, float32 coordinates):
+    order[k] = index of the k-th point along the curve (mbc_spatial_order)."""
+    p = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+    out = np.empty(p.shape[0], np.int32)
+    check(load().mbc_spatial_order(p.shape[0], p.ctypes.data, 3, out.ctypes.data), "mbc_spatial_order")
+    return out
+
+
 def solve_options(**kw) -> _lib.SolveOptions:
     o = _lib.SolveOptions()
     load().mbc_solve_default_options(C.byref(o))

@@ -74,6 +74,7 @@ SIGNATURES = {
     "mbc_plan_get_pattern": (C.c_int, [_vp, _vp, _vp]),
     "mbc_plan_get_supernodes": (C.c_int, [_vp, _vp, _vp, _vp]),
     "mbc_plan_get_factor_pattern": (C.c_int, [_vp, _vp, _vp]),
+    "mbc_spatial_order": (C.c_int, [_i32, _vp, _i32, _vp]),
     "mbc_solver_create": (C.c_int, [_vp, C.POINTER(Operator), _i32, _vp, C.POINTER(_vp)]),
     "mbc_solver_destroy": (C.c_int, [_vp]),
     "mbc_solver_factor": (C.c_int, [_vp, _vp]),

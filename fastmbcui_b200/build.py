@@ -25,7 +25,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr
                      "-Xcompiler", "-fPIC,-fopenmp,-ffp-contract=off", f"-I{INC}", f"-I{CSRC}",
                      "-Xptxas", "-warn-spills"]
 
-HOST_SRC = ["plan.cpp", "capi.cpp"]
+HOST_SRC = ["plan.cpp", "capi.cpp", "spatial.cpp"]
 CUDA_SRC = ["solver.cu", "context.cu", "noalloc.cu", "mlp.cu", "warmstart.cu", "mesh.cu", "int8_ops.cu"]
 
 

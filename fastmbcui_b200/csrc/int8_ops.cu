@@ -23,6 +23,33 @@ bool use_oz(const Solver &S)
   return S.fp64_matvec == MBC_FP64_MATVEC_INT8 && S.oz_ready && S.op.kind == MBC_OP_POINT_KERNEL;
 }
 
+// dst[k, c] = src[idx[k], c] (K x R, FP64): the vector block in the order the
+// planes' reduction axis walks
+__global__ void oz_gather_kernel(int K, int R, const int32_t *__restrict__ idx, const double *__restrict__ src,
+                                 double *__restrict__ dst, const int32_t *__restrict__ done)
+{
+  if (done && *done) return;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)K * R) return;
+  const int k = (int)(t / R), c = (int)(t - (int64_t)k * R);
+  dst[t] = src[(size_t)idx[k] * R + c];
+}
+
+// the coordinates each direction's digit kernel reads: (rows, normals,
+// sources) with the reduction axis in Morton order
+static void oz_coords(const Solver &S, int DIR, const float4 **xr, const float4 **nr, const float4 **ys)
+{
+  if (DIR == 0) {
+    *xr = S.x4();
+    *nr = S.n4();
+    *ys = (const float4 *)S.m_oz_ys.ptr;
+  } else {
+    *xr = (const float4 *)S.m_oz_xr.ptr;
+    *nr = (const float4 *)S.m_oz_nr.ptr;
+    *ys = S.y4();
+  }
+}
+
 template <int NPH>
 static void oz_mma_launch(const oz::OzArgs &a, unsigned grid, cudaStream_t st)
 {
@@ -44,12 +71,16 @@ static int oz_launch(const Solver &S, int R, const double *vin, double *out, con
   const int M = DIR == 0 ? S.nf : S.n;
   const int K = DIR == 0 ? S.n : S.nf;
   const int np = oz::np_for(R), groups = oz::groups_for(R);
-  if (S.m_oz_b.bytes < oz::bimg_bytes(K, R) || S.m_oz_bexp.bytes < sizeof(int32_t) * oz::bexp_count(K, R)) {
+  if (S.m_oz_b.bytes < oz::bimg_bytes(K, R) || S.m_oz_bexp.bytes < sizeof(int32_t) * oz::bexp_count(K, R) ||
+      S.m_oz_v.bytes < sizeof(double) * (size_t)K * R) {
     S.oz_unprepared = true;
     return 0;
   }
+  double *vg = (double *)S.m_oz_v.ptr;
+  oz_gather_kernel<<<(unsigned)cdiv((int64_t)K * R, 256), 256, 0, st>>>(K, R, (const int32_t *)S.m_oz_q[DIR].ptr,
+                                                                       vin, vg, done);
   oz::oz_pack_b_kernel<<<dim3(oz::nchunks_for(K), groups), 512, 0, st>>>(
-      vin, K, R, np, (int8_t *)S.m_oz_b.ptr, S.m_oz_b.bytes, (int32_t *)S.m_oz_bexp.ptr,
+      vg, K, R, np, (int8_t *)S.m_oz_b.ptr, S.m_oz_b.bytes, (int32_t *)S.m_oz_bexp.ptr,
       S.m_oz_bexp.bytes / sizeof(int32_t), done, (int32_t *)S.m_err.ptr);
   oz::OzArgs a{};
   const DevMem &planes = S.oz_slab ? S.m_oz_a[0] : S.m_oz_a[DIR];
@@ -86,15 +117,18 @@ static int oz_launch(const Solver &S, int R, const double *vin, double *out, con
   const int tiles = oz::row_tiles(M);
   if (!S.oz_slab) {
     mma(0, tiles);
-    S.launches += 2;
+    S.launches += 3;
   } else {
     // the planes of each slab of rows, then its products
     const int per = S.oz_slab_tiles[DIR];
     const size_t smem = (DIR == 0 ? 1 : 2) * sizeof(float4) * oz::kChunk;
+    const float4 *cx, *cn, *cy;
+    oz_coords(S, DIR, &cx, &cn, &cy);
+    ++S.launches;  // the gather
     for (int r0 = 0; r0 < tiles; r0 += per) {
       const int cnt = std::min(per, tiles - r0);
       oz::oz_digits_kernel<DIR><<<dim3(oz::nchunks_for(K), cnt), 256, smem, st>>>(
-          S.x4(), S.n4(), S.y4(), S.nf, S.n, (int8_t *)planes.ptr, planes.bytes,
+          cx, cn, cy, S.nf, S.n, (int8_t *)planes.ptr, planes.bytes,
           (int32_t *)S.m_oz_aexp[DIR].ptr, S.m_oz_aexp[DIR].bytes / sizeof(int32_t), r0, oz::kModeDigits, done,
           (int32_t *)S.m_err.ptr);
       mma(r0, cnt);
@@ -167,12 +201,44 @@ mbc_status mbc::Solver::ensure_oz(cudaStream_t st, int R)
       MBC_TRY(m_oz_a[0].reserve(std::max(oz_slab_tiles[0] * t0, oz_slab_tiles[1] * t1)));
       mode = oz::kModeExps;  // exponents of every row now; planes per matvec
     }
+    // Morton order of the sources (K direction: its reduction axis) and of
+    // the collocation rows (K^T direction), and the coordinates in that order
+    {
+      std::vector<float4> hx(nf), hn(nf), hy(n);
+      MBC_CK(cudaMemcpyAsync(hx.data(), x4(), sizeof(float4) * nf, cudaMemcpyDeviceToHost, st));
+      MBC_CK(cudaMemcpyAsync(hn.data(), n4(), sizeof(float4) * nf, cudaMemcpyDeviceToHost, st));
+      MBC_CK(cudaMemcpyAsync(hy.data(), y4(), sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
+      MBC_CK(cudaStreamSynchronize(st));
+      std::vector<int32_t> qs(n), qr(nf);
+      MBC_TRY(spatial_order(n, (const float *)hy.data(), 4, qs.data()));
+      MBC_TRY(spatial_order(nf, (const float *)hx.data(), 4, qr.data()));
+      std::vector<float4> sy(n), sx(nf), sn(nf);
+      for (int k = 0; k < n; ++k) sy[k] = hy[qs[k]];
+      for (int k = 0; k < nf; ++k) {
+        sx[k] = hx[qr[k]];
+        sn[k] = hn[qr[k]];
+      }
+      MBC_TRY(m_oz_q[0].reserve(sizeof(int32_t) * n));
+      MBC_TRY(m_oz_q[1].reserve(sizeof(int32_t) * nf));
+      MBC_TRY(m_oz_ys.reserve(sizeof(float4) * n));
+      MBC_TRY(m_oz_xr.reserve(sizeof(float4) * nf));
+      MBC_TRY(m_oz_nr.reserve(sizeof(float4) * nf));
+      MBC_CK(cudaMemcpyAsync(m_oz_q[0].ptr, qs.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+      MBC_CK(cudaMemcpyAsync(m_oz_q[1].ptr, qr.data(), sizeof(int32_t) * nf, cudaMemcpyHostToDevice, st));
+      MBC_CK(cudaMemcpyAsync(m_oz_ys.ptr, sy.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, st));
+      MBC_CK(cudaMemcpyAsync(m_oz_xr.ptr, sx.data(), sizeof(float4) * nf, cudaMemcpyHostToDevice, st));
+      MBC_CK(cudaMemcpyAsync(m_oz_nr.ptr, sn.data(), sizeof(float4) * nf, cudaMemcpyHostToDevice, st));
+      MBC_CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
+    }
     DevMem &p0 = m_oz_a[0], &p1 = oz_slab ? m_oz_a[0] : m_oz_a[1];
+    const float4 *cx, *cn, *cy;
+    oz_coords(*this, 0, &cx, &cn, &cy);
     oz::oz_digits_kernel<0><<<dim3(oz::nchunks_for(n), oz::row_tiles(nf)), 256, sm0, st>>>(
-        x4(), n4(), y4(), nf, n, (int8_t *)p0.ptr, p0.bytes, (int32_t *)m_oz_aexp[0].ptr,
+        cx, cn, cy, nf, n, (int8_t *)p0.ptr, p0.bytes, (int32_t *)m_oz_aexp[0].ptr,
         m_oz_aexp[0].bytes / sizeof(int32_t), 0, mode, nullptr, (int32_t *)m_err.ptr);
+    oz_coords(*this, 1, &cx, &cn, &cy);
     oz::oz_digits_kernel<1><<<dim3(oz::nchunks_for(nf), oz::row_tiles(n)), 256, sm1, st>>>(
-        x4(), n4(), y4(), nf, n, (int8_t *)p1.ptr, p1.bytes, (int32_t *)m_oz_aexp[1].ptr,
+        cx, cn, cy, nf, n, (int8_t *)p1.ptr, p1.bytes, (int32_t *)m_oz_aexp[1].ptr,
         m_oz_aexp[1].bytes / sizeof(int32_t), 0, mode, nullptr, (int32_t *)m_err.ptr);
     launches += 2;
     MBC_CKL();
@@ -180,11 +246,13 @@ mbc_status mbc::Solver::ensure_oz(cudaStream_t st, int R)
     const int K = std::max(n, nf);
     MBC_TRY(m_oz_b.reserve(oz::bimg_bytes(K, std::max(R, 1))));
     MBC_TRY(m_oz_bexp.reserve(sizeof(int32_t) * oz::bexp_count(K, std::max(R, 1))));
+    MBC_TRY(m_oz_v.reserve(sizeof(double) * (size_t)K * std::max(R, 1)));
     MBC_TRY(oz_selfcheck(st));
   }
   const int K = std::max(n, nf);
   MBC_TRY(m_oz_b.reserve(oz::bimg_bytes(K, R)));
   MBC_TRY(m_oz_bexp.reserve(sizeof(int32_t) * oz::bexp_count(K, R)));
+  MBC_TRY(m_oz_v.reserve(sizeof(double) * (size_t)K * R));
   return MBC_OK;
 }
 

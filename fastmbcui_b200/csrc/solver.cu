@@ -930,62 +930,28 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
     b2 = (const double *)b2ref.ptr;
   }
   const bool compact = o.compact != 0;
-  // With the INT8 FP64 operator every product carries a ~1e-10 relative
-  // error, and the recursive residual drifts from b - A x by the sum of
-  // those errors, which near tol is of the order of tol itself.  The
-  // recursion therefore runs in replacement mode: a column whose recursive
-  // residual reaches its threshold asks for its residual to be recomputed
-  // with the same operator (at the next host check point, for all columns at
-  // once); that residual replaces the recursive one, the search direction is
-  // kept, and the column stops only when the recomputed residual is below
-  // the threshold.  (Restarting from x instead loses the Krylov space: 18 %
-  // more iterations on a 3000-point scene, against a few here.)
-  std::function<mbc_status()> replace_fn;
-  const std::function<mbc_status()> *replace = nullptr;
-  if constexpr (sizeof(T) == 8) {
-    if (oz) {
-      w.sc.drop2 = 1e-300;  // replacement mode, triggered by the threshold alone
-      // replacements come at every check point while columns converge, so
-      // "little progress since the last one" says nothing about stagnation
-      w.sc.stall_check = 0;
-      const Layout2D L = layout2d(n, R);
-      replace_fn = [&, L]() -> mbc_status {
-        if (adjoint) {
-          launch_rows<T>(*this, R, w.X, w.W, nullptr, st);
-          launch_cols<T>(*this, R, w.W, w.Z, nullptr, nullptr, nullptr, st);
-          sub_kernel<T><<<cdiv(nv, 256), 256, 0, st>>>(nv, (const T *)fm.ptr, w.Z, w.Rv);
-          ++launches;
-        } else {
-          residual<T>(*this, R, (const T *)fm.ptr, w.X, w.W, w.Rv, st);
-        }
-        dot_partial_kernel<T><<<L.grid, L.block, L.smem, st>>>(n, R, w.Rv, w.Rv, w.part);
-        reduce_kernel<<<1, 1024, 0, st>>>((int)L.grid.x, R, w.part, RED_REPLACE, w.sc, nullptr);
-        launches += 2;
-        MBC_CKL();
-        return MBC_OK;
-      };
-      replace = &replace_fn;
-    }
-  }
-  const int max_replace = replace ? std::max(1, o.max_iters / std::max(1, o.check_every) + 1) : 0;
   if (precision == MBC_F64)
     MBC_TRY((run_pcg<T, double, T>(*this, R, w, w.X, (const double *)lval.ptr, o.max_iters, o.tol,
                                    o.precondition != 0, std::max(1, o.check_every), nullptr, st, b2,
-                                   replace, max_replace, compact)));
+                                   nullptr, 0, compact)));
   else
     MBC_TRY((run_pcg<T, float, T>(*this, R, w, w.X, (const float *)lval.ptr, o.max_iters, o.tol,
                                   o.precondition != 0, std::max(1, o.check_every), nullptr, st, b2,
-                                  replace, max_replace, compact)));
+                                  nullptr, 0, compact)));
   std::vector<int32_t> status, iters;
   std::vector<double> rel;
   MBC_TRY(collect<T>(*this, R, w, status, iters, rel, st));
   if constexpr (sizeof(T) == 8) {
     if (oz) {
-      // The INT8 FP64 operator carries a ~1e-10 relative error, so the
-      // recursive residual can end slightly above tol once recomputed with
-      // the same operator (1.3e-8 for 1e-8 after ~270 iterations in
-      // emulation).  Every column is decided on that recomputed residual, and
-      // those above tol restart from where they stand, at most twice.
+      // The INT8 FP64 operator carries a ~1e-9 relative error (measured on
+      // the B200 at the solution), so the recursive residual can end above
+      // tol once recomputed with the same operator; that recomputed residual
+      // agrees with the FP64 one to ~1e-3 relative.  Every column is decided
+      // on it, and those above tol restart from where they stand, at most
+      // twice.  A restart builds a fresh Krylov space from the accurate
+      // residual; replacing the residual inside the recursion instead stalls
+      // the ill-conditioned columns (measured: 544 against 179 iterations on
+      // one column of a 3000-point scene).
       T *bvec = w.Tt;
       if (adjoint) MBC_CK(cudaMemcpyAsync(bvec, fm.ptr, sizeof(T) * nv, cudaMemcpyDeviceToDevice, st));
       else launch_cols<T>(*this, R, (const T *)fm.ptr, bvec, nullptr, nullptr, nullptr, st);

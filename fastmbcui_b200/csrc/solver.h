@@ -55,6 +55,12 @@ struct Solver {
   // (0: rows, 1: columns), and the per-launch digit image of the vector block
   DevMem m_oz_a[2], m_oz_aexp[2];
   mutable DevMem m_oz_b, m_oz_bexp;
+  // the reduction axes of the INT8 planes walk the points in Morton order:
+  // m_oz_q[0][k] = plan position of the k-th source (K direction), m_oz_q[1][k]
+  // = the k-th collocation row (K^T direction); the coordinates in that
+  // order; the vector block gathered into it for each matvec
+  DevMem m_oz_q[2], m_oz_ys, m_oz_xr, m_oz_nr;
+  mutable DevMem m_oz_v;
   DevMem m_oz_chk;  // the self-check's vectors
   // factor
   DevMem theta, theta64, lval, bad, fscratch;

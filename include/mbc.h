@@ -92,6 +92,14 @@ mbc_status mbc_plan_get_supernodes(const mbc_plan *plan, int32_t *sup_ptr_host,
 mbc_status mbc_plan_get_factor_pattern(const mbc_plan *plan, int32_t *lptr_host,
                                        int32_t *lind_host);
 
+/* Morton (Z-curve) order of n points: order_host[k] = index of the k-th point
+ * along the curve (21 bits per axis over the points' bounding cube, ties by
+ * index).  Coordinates at pts_host[i * stride + 0..2], stride >= 3 floats.
+ * No counterpart in the reference: the INT8 FP64 matvec walks its reduction
+ * axes in this order (mbc_solver_set_fp64_matvec), and tests use it to
+ * restate that matvec. */
+mbc_status mbc_spatial_order(int32_t n, const float *pts_host, int32_t stride, int32_t *order_host);
+
 /* ------------------------------------------------------------------------ */
 /* Operator K (nf collocation rows x n source columns).                       */
 /* ------------------------------------------------------------------------ */

@@ -66,6 +66,10 @@ class Case:
         self.P = P.astype(np.int64)
         self.Pinv = np.argsort(self.P)
         self.G = _G(sc)
+        # the planes' reduction axes walk the sources (K) and the rows (K^T)
+        # in Morton order; the sources are given to it in plan order
+        self.ks = self.Pinv[F.spatial_order(sc.y[self.Pinv])]  # original source indices along K's axis
+        self.kr = F.spatial_order(sc.x).astype(np.int64)      # row indices along K^T's axis
 
 
 @pytest.fixture(scope="module")
@@ -80,7 +84,7 @@ def test_apply_K(case, R):
     V = np.random.default_rng(R).standard_normal((sc.n, R))
     W8 = case.s8.apply_K(_dev(V)).cpu().numpy().reshape(sc.nf, R)
     W64 = case.s64.apply_K(_dev(V)).cpu().numpy().reshape(sc.nf, R)
-    Gn, Vn = case.G[:, case.Pinv], V[case.Pinv]  # the device's source order
+    Gn, Vn = case.G[:, case.ks], V[case.ks]  # the device's reduction order
     Wo = O.oz_apply(Gn, Vn, coef=sc.coef)
     bound = _bound(Gn, Vn, sc.coef)
     assert np.all(np.abs(W8 - Wo) <= bound / 64)
@@ -95,9 +99,10 @@ def test_apply_KT(case, R):
     W = np.random.default_rng(100 + R).standard_normal((sc.nf, R))
     T8 = case.s8.apply_KT(_dev(W)).cpu().numpy().reshape(sc.n, R)
     T64 = case.s64.apply_KT(_dev(W)).cpu().numpy().reshape(sc.n, R)
-    GnT = np.ascontiguousarray(case.G[:, case.Pinv].T)  # sources (device order) x rows
-    To = O.oz_apply(GnT, W, coef=sc.coef)[case.P]      # back to the original order
-    bound = _bound(GnT, W, sc.coef)[case.P]
+    GnT = np.ascontiguousarray(case.G[case.kr][:, case.Pinv].T)  # sources (plan order) x rows (Morton)
+    Wk = W[case.kr]
+    To = O.oz_apply(GnT, Wk, coef=sc.coef)[case.P]               # back to the original order
+    bound = _bound(GnT, Wk, sc.coef)[case.P]
     assert np.all(np.abs(T8 - To) <= bound / 64)
     assert np.all(np.abs(T8 - T64) <= bound)
     assert np.linalg.norm(T8 - T64) / np.linalg.norm(T64) <= 1e-9
