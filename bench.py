@@ -228,7 +228,8 @@ def run_trajectory(args):
         warm = _learned_start(args, base, q, scenes, dev)
     mode = {"mixed64": "mixed", "mixed": "fp32-replace"}.get(args.solver, args.solver)
     ts = TrajectorySolver(base.coef, mode=mode, fp64_matvec=args.fp64_matvec, warm=warm,
-                          max_iters=args.max_iters, compact=args.compact, matvec=MATVEC[args.matvec])
+                          max_iters=args.max_iters, compact=args.compact, matvec=MATVEC[args.matvec],
+                          schedule=args.schedule)
     cold = None
     for k in range(args.warmup):
         if callable(warm):
@@ -302,7 +303,7 @@ def run_trajectory(args):
         "data": "synthetic (seeded trajectory)",
         "config": {"workload": "trajectory32", "desc": WORKLOADS["trajectory32"][1], "N": base.n,
                    "Nf": base.nf, "R": R, "rho": base.rho, "lambda": base.lam, "tol": 1e-8,
-                   "precision": PRECISION[args.solver], "schedule": "batched",
+                   "precision": PRECISION[args.solver], "schedule": SCHEDULE[args.schedule],
                    "warm_start": WARM[args.warm],
                    "steps_requested": args.steps, "steps_run": len(times),
                    "plan_every": args.plan_every, "solver": args.solver, "fp64_matvec": args.fp64_matvec,
@@ -348,6 +349,8 @@ PRECISION = {"flexible": "FP64 flexible CG around FP32 PCG",
              "mixed64": "FP32 factor and preconditioner (FP64 retry of cancelling supernodes); FP64 PCG "
                         "vectors, dots and scalars; FP64-accurate matvec",
              "mixed": "FP32 PCG recursion with FP64 residual replacement and FP64 polish"}
+SCHEDULE = {"block": "block PCG over all columns (shared Krylov space, per-column stopping)",
+            "batched": "batched PCG (per-column recurrences advanced together)"}
 WARM = {"learned": "quadratic extrapolation + MLP correction (3x256, BF16 weights)",
         "extrapolate": "quadratic extrapolation of the last three steps' strengths",
         "previous": "previous step's strengths", "cold": "x0 = 0"}
@@ -1096,6 +1099,8 @@ def main():
                     help="with --kernel-probe: one full mixed solve instead of K / K^T launches")
     ap.add_argument("--matvec", default="auto", choices=sorted(MATVEC),
                     help="FP32 matvec: tensor cores (3xTF32 tcgen05) or CUDA cores")
+    ap.add_argument("--schedule", default="block", choices=["block", "batched"],
+                    help="trajectory: block PCG (the columns share one Krylov space) or batched PCG")
     ap.add_argument("--compact", action="store_true",
                     help="FP64 solves: continue on the still-active columns alone once at most half remain")
     ap.add_argument("--rows-probe", action="store_true",

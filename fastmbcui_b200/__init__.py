@@ -13,12 +13,12 @@ import numpy as np
 from . import _lib
 from ._lib import (MBC_F32, MBC_F64, MBC_FP64_MATVEC_INT8, MBC_FP64_MATVEC_SIMT, MBC_MATVEC_AUTO,
                    MBC_MATVEC_SIMT, MBC_MATVEC_TENSOR,
-                   MBC_OP_DENSE, MBC_OP_POINT_KERNEL, MBC_SCHED_BATCHED, MBC_SCHED_PER_RHS, MbcError,
+                   MBC_OP_DENSE, MBC_OP_POINT_KERNEL, MBC_SCHED_BATCHED, MBC_SCHED_PER_RHS, MBC_SCHED_BLOCK, MbcError,
                    check, ptr)
 
 __all__ = ["Plan", "Solver", "MbcError", "load", "plan_many", "solve_many", "MBC_F32", "MBC_F64",
            "MBC_SCHED_BATCHED",
-           "MBC_SCHED_PER_RHS", "MBC_MATVEC_AUTO", "MBC_MATVEC_SIMT", "MBC_MATVEC_TENSOR",
+           "MBC_SCHED_PER_RHS", "MBC_SCHED_BLOCK", "MBC_MATVEC_AUTO", "MBC_MATVEC_SIMT", "MBC_MATVEC_TENSOR",
            "MBC_FP64_MATVEC_SIMT", "MBC_FP64_MATVEC_INT8"]
 
 

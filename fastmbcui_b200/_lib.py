@@ -18,7 +18,7 @@ MBC_OK, MBC_NOT_CONVERGED, MBC_BREAKDOWN, MBC_NONSPD_PIVOT, MBC_BAD_ARG = 0, 1, 
 MBC_CUDA_ERROR, MBC_TIMEOUT, MBC_NO_MEMORY, MBC_COVERAGE, MBC_UNSUPPORTED = 5, 6, 7, 8, 9
 MBC_F64, MBC_F32 = 0, 1
 MBC_OP_DENSE, MBC_OP_POINT_KERNEL = 0, 1
-MBC_SCHED_BATCHED, MBC_SCHED_PER_RHS = 0, 1
+MBC_SCHED_BATCHED, MBC_SCHED_PER_RHS, MBC_SCHED_BLOCK = 0, 1, 2
 MBC_MATVEC_AUTO, MBC_MATVEC_SIMT, MBC_MATVEC_TENSOR = 0, 1, 2
 MBC_FP64_MATVEC_SIMT, MBC_FP64_MATVEC_INT8 = 0, 1
 

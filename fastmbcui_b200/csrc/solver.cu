@@ -13,6 +13,7 @@
 
 #include <cuda_runtime.h>
 
+#include "block.cuh"
 #include "factor.cuh"
 #include "forces.cuh"
 #include "matvec.cuh"
@@ -758,6 +759,220 @@ static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, XT *x, const LT *lval
   return MBC_OK;
 }
 
+// Block PCG: the outcome of one step for the active columns act[0 .. a) of
+// the caller's batch: rr = |r|^2 (FP64), iteration count, converge / max
+// iterations / breakdown (NaN) tests against each column's threshold.
+__global__ void block_check_kernel(int a, const int32_t *__restrict__ act, const double *__restrict__ rr,
+                                   PcgScalars sc)
+{
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a) return;
+  const int c = act[j];
+  if (sc.status[c] != COL_ACTIVE) return;
+  const double s = rr[j];
+  sc.rr[c] = s;
+  sc.iters[c] += 1;
+  if (!(s == s)) sc.status[c] = COL_BREAKDOWN;
+  else if (s < sc.thr[c]) sc.status[c] = COL_OK;
+  else if (sc.iters[c] >= sc.maxit) sc.status[c] = COL_MAXIT;
+}
+
+// every column in act[0 .. a) still active gets status `st` (a breakdown of the block step)
+__global__ void block_fail_kernel(int a, const int32_t *__restrict__ act, PcgScalars sc, int32_t st)
+{
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < a && sc.status[act[j]] == COL_ACTIVE) sc.status[act[j]] = st;
+}
+
+// Block PCG on (K^T K) X = B for R columns (schedule MBC_SCHED_BLOCK):
+// O'Leary's block conjugate gradients with the KL preconditioner, search
+// blocks kept orthonormal (rank-revealing Cholesky QR, twice; block.cuh).
+// All active columns share one Krylov space, so a column whose own Krylov
+// space converges slowly is helped by the directions the other columns
+// found.  One step, for the active columns (compact, n x a):
+//   Q = A P;  G = P^T Q;  alpha = G^-1 P^T R;  X += P alpha;  R -= Q alpha;
+//   per-column stop test on |r|^2 (the thresholds of the batched PCG);
+//   Z = M R (still active columns);  beta = -G^-1 Q^T Z;
+//   P = orth(Z + P beta).
+// Columns leave the block as they converge (their X goes back to w.X), so
+// the matvec and the dense products shrink with the active set.  On entry
+// w.X holds x0 and w.Rv the residual b - A x0 (new order, n x R); on exit
+// w.X holds the solutions and w.sc the per-column status, iterations and
+// |r|^2.  FP64 throughout (the matvec per the solver's FP64 choice).
+template <typename LT>
+static mbc_status run_block_pcg(Solver &S, int R, PcgWork<double> &w, const LT *lval, int maxit, double tol,
+                                const double *d_b2ref, cudaStream_t st)
+{
+  const int n = S.n;
+  if (R > blk::kOrthMax) return fail(MBC_UNSUPPORTED, "block PCG: more than 512 columns");
+  const Layout2D L0 = layout2d(n, R);
+  w.sc.maxit = maxit;
+  w.sc.tol2 = tol * tol;
+  set_status_kernel<<<cdiv(R, 256), 256, 0, st>>>(R, w.sc.status, w.sc.iters, w.sc.done, w.sc.want, w.sc.rz,
+                                                   nullptr);
+  dot_partial_kernel<double><<<L0.grid, L0.block, L0.smem, st>>>(n, R, w.Rv, w.Rv, w.part);
+  reduce_kernel<<<1, 1024, 0, st>>>((int)L0.grid.x, R, w.part, RED_INIT_B, w.sc, nullptr);
+  if (d_b2ref) set_thresholds_kernel<<<cdiv(R, 256), 256, 0, st>>>(R, w.sc.tol2, d_b2ref, w.sc);
+  S.launches += d_b2ref ? 4 : 3;
+  MBC_CKL();
+  // device memory: compact X / R (two sets), search blocks P and V, small
+  // matrices (ld R), Gram partials, index lists
+  const size_t nv = (size_t)n * R, sm = (size_t)R * R;
+  const int chunks = blk::gram_chunks(n);
+  const size_t bytes = sizeof(double) * (6 * nv + 6 * sm + (size_t)chunks * sm + R) + sizeof(int32_t) * (3 * R + 8);
+  MBC_TRY(S.blk.reserve(bytes));
+  double *base = (double *)S.blk.ptr;
+  double *Xa[2] = {base, base + nv}, *Ra[2] = {base + 2 * nv, base + 3 * nv};
+  double *P = base + 4 * nv, *V = base + 5 * nv;
+  double *G = base + 6 * nv, *Sm = G + sm, *H = Sm + sm, *Wm = H + sm, *T1 = Wm + sm, *T2 = T1 + sm;
+  double *gpart = T2 + sm, *rr = gpart + (size_t)chunks * sm;
+  int32_t *d_act = (int32_t *)(rr + R), *d_loc = d_act + R, *d_perm = d_loc + R, *d_small = d_perm + R;
+  double *Q = w.Tt, *Z = w.Z, *U = w.U, *W = w.W;
+  // host view
+  std::vector<int32_t> status(R), act, loc;
+  int32_t *h_small = S.h_flag;  // pinned: [rank, flag]
+  auto gram = [&](const double *A, int lda, int ka, const double *B, int ldb, int kb, double *C) {
+    const dim3 g((unsigned)chunks, cdiv(ka, blk::kTile), cdiv(kb, blk::kTile));
+    blk::gram_partial_kernel<<<g, blk::kThreads, 0, st>>>(n, A, lda, ka, B, ldb, kb, gpart);
+    blk::gram_reduce_kernel<<<cdiv((int64_t)ka * kb, 256), 256, 0, st>>>(chunks, ka, kb, gpart, C, R);
+    S.launches += 2;
+  };
+  auto update = [&](int k, int m, const double *Pm, int ldp, const double *M, const double *bse, int ldb,
+                    double sgn, double *out, int ldo, const int32_t *skip = nullptr) {
+    const dim3 g(cdiv(n, blk::kTile), cdiv(m, blk::kTile));
+    blk::block_update_kernel<<<g, blk::kThreads, 0, st>>>(n, k, m, Pm, ldp, M, R, bse, ldb, sgn, out, ldo, skip);
+    ++S.launches;
+  };
+  auto precond = [&](int a, const double *Rm, double *Zm) {
+    const Layout2D La = layout2d(n, a);
+    precond_lt_kernel<double, LT><<<La.grid, La.block, 0, st>>>(n, a, S.d_lptr(), S.d_lind(), lval, Rm, U, nullptr);
+    precond_l_kernel<double, LT><<<La.grid, La.block, La.smem, st>>>(n, a, S.d_rptr(), S.d_rcol(), S.d_rmap(), lval,
+                                                                      U, Zm, Rm, w.part, nullptr);
+    S.launches += 2;
+  };
+  // P (n x r, ld r) = an orthonormal basis of the columns of Vin (n x m, ld
+  // m; Vin is P's partner buffer V or Z, not needed afterwards), dependent
+  // directions dropped; r = 0 when none is left.  Pass 1 writes P, pass 2 V,
+  // then P and V swap.
+  auto orth = [&](const double *Vin, int m, int *r_out) -> mbc_status {
+    gram(Vin, m, m, Vin, m, m, Wm);
+    blk::orth_factor_kernel<<<1, blk::kSmallThreads, 0, st>>>(m, Wm, R, 1e-6, T1, R, d_perm, d_small);
+    MBC_CK(cudaMemcpyAsync(h_small, d_small, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    MBC_CK(cudaStreamSynchronize(st));
+    const int r = h_small[0];
+    ++S.launches;
+    *r_out = r;
+    if (r == 0) return MBC_OK;
+    update(m, r, Vin, m, T1, nullptr, 0, 1.0, P, r);
+    // second pass: the first leaves an orthogonality error of order
+    // eps cond^2, which the second removes (cond <= 1e6 after the drop)
+    gram(P, r, r, P, r, r, Wm);
+    blk::orth_factor_kernel<<<1, blk::kSmallThreads, 0, st>>>(r, Wm, R, 0.0, T2, R, d_perm, d_small);
+    MBC_CK(cudaMemcpyAsync(h_small, d_small, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    MBC_CK(cudaStreamSynchronize(st));
+    const int r2 = h_small[0];
+    ++S.launches;
+    *r_out = r2;
+    if (r2 == 0) return MBC_OK;
+    update(r, r2, P, r, T2, nullptr, 0, 1.0, V, r2);
+    std::swap(P, V);
+    return MBC_OK;
+  };
+  // the active columns, gathered into the compact block
+  MBC_CK(cudaMemcpyAsync(status.data(), w.sc.status, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, st));
+  MBC_CK(cudaStreamSynchronize(st));
+  for (int c = 0; c < R; ++c)
+    if (status[c] == COL_ACTIVE) act.push_back(c);
+  int a = (int)act.size();
+  if (a == 0) return MBC_OK;
+  int cur = 0;
+  MBC_CK(cudaMemcpyAsync(d_act, act.data(), sizeof(int32_t) * a, cudaMemcpyHostToDevice, st));
+  gather_cols_kernel<double><<<cdiv((int64_t)n * a, 256), 256, 0, st>>>(n, R, a, d_act, w.X, Xa[cur]);
+  gather_cols_kernel<double><<<cdiv((int64_t)n * a, 256), 256, 0, st>>>(n, R, a, d_act, w.Rv, Ra[cur]);
+  S.launches += 2;
+  precond(a, Ra[cur], Z);
+  int k = 0;
+  MBC_TRY(orth(Z, a, &k));
+  if (S.profile) MBC_TRY(S.ensure_events(2));
+  int32_t *d_flag = d_small + 1;
+  bool failed = false;
+  for (int it = 0; it < maxit && k > 0; ++it) {
+    if (S.profile) MBC_CK(cudaEventRecord(S.events[0], st));
+    launch_rows<double>(S, k, P, W, nullptr, st);
+    launch_cols<double>(S, k, W, Q, nullptr, nullptr, nullptr, st);
+    if (S.profile) MBC_CK(cudaEventRecord(S.events[1], st));
+    // alpha = (P^T A P)^-1 P^T R;  X += P alpha;  R -= Q alpha
+    gram(P, k, k, Q, k, k, G);
+    gram(P, k, k, Ra[cur], a, a, Sm);
+    MBC_CK(cudaMemsetAsync(d_flag, 0, sizeof(int32_t), st));
+    blk::chol_kernel<<<1, blk::kSmallThreads, 0, st>>>(k, G, R, d_flag);
+    blk::chol_solve_kernel<<<1, blk::kSmallThreads, 0, st>>>(k, G, R, a, Sm, R, 1.0, d_flag);
+    update(k, a, P, k, Sm, Xa[cur], a, 1.0, Xa[cur], a, d_flag);
+    update(k, a, Q, k, Sm, Ra[cur], a, -1.0, Ra[cur], a, d_flag);
+    // per-column stop test on |r|^2
+    const Layout2D La = layout2d(n, a);
+    dot_partial_kernel<double><<<La.grid, La.block, La.smem, st>>>(n, a, Ra[cur], Ra[cur], w.part);
+    PcgScalars none{};
+    reduce_kernel<<<1, 1024, 0, st>>>((int)La.grid.x, a, w.part, RED_STORE, none, rr);
+    block_check_kernel<<<cdiv(a, 256), 256, 0, st>>>(a, d_act, rr, w.sc);
+    S.launches += 6;
+    MBC_CKL();
+    MBC_CK(cudaMemcpyAsync(status.data(), w.sc.status, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, st));
+    MBC_CK(cudaMemcpyAsync(h_small + 1, d_flag, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    MBC_CK(cudaStreamSynchronize(st));
+    if (S.profile) {
+      float ms = 0.f;
+      MBC_CK(cudaEventElapsedTime(&ms, S.events[0], S.events[1]));
+      S.prof_ms_all.push_back(ms);
+      S.prof_is64.push_back(1);
+    }
+    if (h_small[1]) {  // P^T A P not positive definite (NaN or breakdown): nothing was updated
+      failed = true;
+      break;
+    }
+    std::vector<int32_t> keep;  // positions in the compact block of the columns still active
+    for (int j = 0; j < a; ++j)
+      if (status[act[j]] == COL_ACTIVE) keep.push_back(j);
+    const int a2 = (int)keep.size();
+    if (a2 < a) {
+      // finished columns' x back to the batch (the others are rewritten later)
+      scatter_cols_kernel<double><<<cdiv((int64_t)n * a, 256), 256, 0, st>>>(n, R, a, d_act, Xa[cur], w.X);
+      ++S.launches;
+      if (a2 == 0) {
+        a = 0;
+        break;
+      }
+      MBC_CK(cudaMemcpyAsync(d_loc, keep.data(), sizeof(int32_t) * a2, cudaMemcpyHostToDevice, st));
+      gather_cols_kernel<double><<<cdiv((int64_t)n * a2, 256), 256, 0, st>>>(n, a, a2, d_loc, Xa[cur], Xa[cur ^ 1]);
+      gather_cols_kernel<double><<<cdiv((int64_t)n * a2, 256), 256, 0, st>>>(n, a, a2, d_loc, Ra[cur], Ra[cur ^ 1]);
+      S.launches += 2;
+      std::vector<int32_t> act2(a2);
+      for (int j = 0; j < a2; ++j) act2[j] = act[keep[j]];
+      act.swap(act2);
+      MBC_CK(cudaMemcpyAsync(d_act, act.data(), sizeof(int32_t) * a2, cudaMemcpyHostToDevice, st));
+      cur ^= 1;
+      a = a2;
+    }
+    // next search block: P = orth(Z + P beta), beta = -(P^T A P)^-1 Q^T Z
+    precond(a, Ra[cur], Z);
+    gram(Q, k, k, Z, a, a, H);
+    blk::chol_solve_kernel<<<1, blk::kSmallThreads, 0, st>>>(k, G, R, a, H, R, -1.0, nullptr);
+    update(k, a, P, k, H, Z, a, 1.0, V, a);
+    S.launches += 1;
+    MBC_TRY(orth(V, a, &k));
+  }
+  if (a > 0) {
+    // out of iterations, no search direction left, or a failed step: the
+    // columns still active end as not converged (their x as it stands)
+    scatter_cols_kernel<double><<<cdiv((int64_t)n * a, 256), 256, 0, st>>>(n, R, a, d_act, Xa[cur], w.X);
+    block_fail_kernel<<<cdiv(a, 256), 256, 0, st>>>(a, d_act, w.sc, COL_MAXIT);
+    S.launches += 2;
+    MBC_CKL();
+  }
+  (void)failed;
+  return MBC_OK;
+}
+
 // residual r = K^T (f - K x) in T, all columns; f, x new-order buffers
 template <typename T>
 static void residual(Solver &S, int R, const T *F, const T *X, T *W, T *Rout, cudaStream_t st)
@@ -930,28 +1145,44 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
     b2 = (const double *)b2ref.ptr;
   }
   const bool compact = o.compact != 0;
-  if (precision == MBC_F64)
-    MBC_TRY((run_pcg<T, double, T>(*this, R, w, w.X, (const double *)lval.ptr, o.max_iters, o.tol,
+  // block PCG (FP64 recursions only; the preconditioner is always applied)
+  const bool block = sizeof(T) == 8 && o.schedule == MBC_SCHED_BLOCK && R > 1;
+  // The INT8 operator's recomputed residual can read up to ~10 % below the
+  // FP64 one near tol (measured at N = 64000), so its columns are run and
+  // decided against 0.85 tol.
+  const double rtol = oz ? 0.85 * o.tol : o.tol;
+  if (block) {
+    if constexpr (sizeof(T) == 8) {
+      PcgWork<double> &wd = reinterpret_cast<PcgWork<double> &>(w);
+      if (precision == MBC_F64)
+        MBC_TRY(run_block_pcg<double>(*this, R, wd, (const double *)lval.ptr, o.max_iters, rtol, b2, st));
+      else
+        MBC_TRY(run_block_pcg<float>(*this, R, wd, (const float *)lval.ptr, o.max_iters, rtol, b2, st));
+    }
+  } else if (precision == MBC_F64) {
+    MBC_TRY((run_pcg<T, double, T>(*this, R, w, w.X, (const double *)lval.ptr, o.max_iters, rtol,
                                    o.precondition != 0, std::max(1, o.check_every), nullptr, st, b2,
                                    nullptr, 0, compact)));
-  else
-    MBC_TRY((run_pcg<T, float, T>(*this, R, w, w.X, (const float *)lval.ptr, o.max_iters, o.tol,
+  } else {
+    MBC_TRY((run_pcg<T, float, T>(*this, R, w, w.X, (const float *)lval.ptr, o.max_iters, rtol,
                                   o.precondition != 0, std::max(1, o.check_every), nullptr, st, b2,
                                   nullptr, 0, compact)));
+  }
   std::vector<int32_t> status, iters;
   std::vector<double> rel;
   MBC_TRY(collect<T>(*this, R, w, status, iters, rel, st));
   if constexpr (sizeof(T) == 8) {
-    if (oz) {
+    if (oz || block) {
       // The INT8 FP64 operator carries a ~1e-9 relative error (measured on
-      // the B200 at the solution), so the recursive residual can end above
-      // tol once recomputed with the same operator; that recomputed residual
-      // agrees with the FP64 one to ~1e-3 relative.  Every column is decided
-      // on it, and those above tol restart from where they stand, at most
-      // twice.  A restart builds a fresh Krylov space from the accurate
-      // residual; replacing the residual inside the recursion instead stalls
-      // the ill-conditioned columns (measured: 544 against 179 iterations on
-      // one column of a 3000-point scene).
+      // the B200 at the solution), and the block recursion's residual drifts
+      // further from the true one than a single column's, so the recursive
+      // residual can end above tol once recomputed.  Every column is decided
+      // on its residual recomputed with the solver's operator, and those
+      // above the threshold restart (batched per-column PCG) from where they
+      // stand, at most twice.  A restart builds a fresh Krylov space from the
+      // accurate residual; replacing the residual inside the recursion
+      // instead stalls the ill-conditioned columns (measured: 544 against 179
+      // iterations on one column of a 3000-point scene).
       T *bvec = w.Tt;
       if (adjoint) MBC_CK(cudaMemcpyAsync(bvec, fm.ptr, sizeof(T) * nv, cudaMemcpyDeviceToDevice, st));
       else launch_cols<T>(*this, R, (const T *)fm.ptr, bvec, nullptr, nullptr, nullptr, st);
@@ -974,7 +1205,7 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
         for (int c = 0; c < R; ++c) {
           rel[c] = nb[c] < 1e-16 ? 0.0 : std::sqrt(nr[c] / nb[c]);
           if (status[c] == COL_BREAKDOWN) continue;
-          status[c] = rel[c] <= o.tol ? COL_OK : COL_MAXIT;
+          status[c] = rel[c] <= rtol ? COL_OK : COL_MAXIT;
           if (status[c] == COL_MAXIT) pol.push_back(c);
         }
         if (pol.empty() || pass == 2) break;
@@ -996,11 +1227,11 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
         launches += 2;
         MBC_CKL();
         if (precision == MBC_F64)
-          MBC_TRY((run_pcg<T, double, T>(*this, Rs, ws, ws.X, (const double *)lval.ptr, o.max_iters, o.tol,
+          MBC_TRY((run_pcg<T, double, T>(*this, Rs, ws, ws.X, (const double *)lval.ptr, o.max_iters, rtol,
                                          o.precondition != 0, std::max(1, o.check_every), nullptr, st, d_b2s,
                                          nullptr, 0, compact)));
         else
-          MBC_TRY((run_pcg<T, float, T>(*this, Rs, ws, ws.X, (const float *)lval.ptr, o.max_iters, o.tol,
+          MBC_TRY((run_pcg<T, float, T>(*this, Rs, ws, ws.X, (const float *)lval.ptr, o.max_iters, rtol,
                                         o.precondition != 0, std::max(1, o.check_every), nullptr, st, d_b2s,
                                         nullptr, 0, compact)));
         std::vector<int32_t> it2(Rs);

@@ -66,6 +66,7 @@ struct Solver {
   DevMem theta, theta64, lval, bad, fscratch;
   // PCG workspaces
   DevMem work32, work64, part, scal, fbuf32, fbuf64, res64, mask, colbuf, tmp, b2ref, nrm, polish_idx;
+  DevMem blk;  // block PCG: compact column blocks, search blocks, small matrices
 
   ~Solver();
 

@@ -19,6 +19,11 @@ Precision modes (``mode``):
   "fp32-replace"  FP32 recursion (tensor-core 3xTF32 matvec) with FP64
            residual replacement and an FP64 polish of stagnating columns.
 
+Schedules (``schedule``): "block" (block PCG: the columns share one Krylov
+space, so slowly converging columns borrow the directions the others found;
+"mixed" and "fp64" modes) or "batched" (independent per-column recurrences
+advanced together).
+
 Warm starts (``warm``): "extrapolate" (quadratic extrapolation of the last
 three steps' strengths, linear with two, the previous with one), "previous",
 "cold" (x0 = 0), or a callable ``warm(history) -> X0 or None``.
@@ -26,7 +31,7 @@ Every column is still decided on its own FP64 residual, whatever the start.
 """
 from __future__ import annotations
 
-from . import MBC_F32, MBC_F64, Solver
+from . import MBC_F32, MBC_F64, MBC_SCHED_BATCHED, MBC_SCHED_BLOCK, Solver
 
 MODES = ("mixed", "fp64", "fp32-replace")
 
@@ -45,12 +50,13 @@ def extrapolate(hist):
 class TrajectorySolver:
     def __init__(self, coef: float, *, mode: str = "mixed", fp64_matvec: str = "int8",
                  warm="extrapolate", tol: float = 1e-8, max_iters: int = 3000, check_every: int = 8,
-                 compact: bool = False, matvec: int = 0):
+                 compact: bool = False, matvec: int = 0, schedule: str = "block"):
         if mode not in MODES:
             raise ValueError(f"mode must be one of {MODES}")
         self.coef, self.mode, self.fp64_matvec = float(coef), mode, fp64_matvec
         self.warm, self.tol, self.max_iters = warm, float(tol), int(max_iters)
         self.check_every, self.compact, self.matvec = int(check_every), bool(compact), int(matvec)
+        self.schedule = {"block": MBC_SCHED_BLOCK, "batched": MBC_SCHED_BATCHED}[schedule]
         self.history = []
 
     def start(self):
@@ -90,7 +96,7 @@ class TrajectorySolver:
             X, st = s.solve(F, out_dtype=torch.float32, max_refine=64, inner_tol=1e-2,
                             compact=int(self.compact), **opts)
         else:
-            X, st = s.solve(F, out_dtype=torch.float64, compact=int(self.compact),
+            X, st = s.solve(F, out_dtype=torch.float64, compact=int(self.compact), schedule=self.schedule,
                             fp64_recursion=1 if self.mode == "mixed" else 0, **opts)
         if keep:
             self.history = (self.history + [X])[-3:]

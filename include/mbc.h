@@ -181,7 +181,10 @@ mbc_status mbc_solver_prepare(mbc_solver *s, mbc_stream stream);
 
 typedef enum {
   MBC_SCHED_BATCHED = 0, /* all R columns advance together (per-column alpha, beta, stop) */
-  MBC_SCHED_PER_RHS = 1  /* one cold-started PCG per column, in order (the reference's loop) */
+  MBC_SCHED_PER_RHS = 1, /* one cold-started PCG per column, in order (the reference's loop) */
+  MBC_SCHED_BLOCK = 2    /* block PCG: all active columns share one Krylov space (FP64 recursions:
+                            MBC_F64 solvers, or MBC_F32 with fp64_recursion; at most 512 columns);
+                            every column still stops on its own residual */
 } mbc_schedule;
 
 typedef struct {
