@@ -205,7 +205,7 @@ def run_trajectory(args):
     nsteps = args.warmup + args.steps
     n_e2e = max(1, args.e2e_steps)
     t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
-    scenes = [S.moved(base, q[k]) for k in range(nsteps + n_e2e)]
+    scenes = [S.moved(base, q[k]) for k in range(nsteps + n_e2e + 1)]  # + the ablation's pose
     # the host plan of each step; with --plan-every K (an opt-in mode that is
     # not the plain method) the ordering, pattern and supernodes of a step are
     # reused for the next K - 1 steps and only the factor is rebuilt, on the
@@ -332,8 +332,9 @@ def run_trajectory(args):
         if out["plain_fp64"].get("solves_per_s"):
             out["speedup_vs_plain_fp64"] = round(value / out["plain_fp64"]["solves_per_s"], 2)
     if args.ablation and _left(args) > args.reserve_s * 0.35:
-        out["ablation"] = _ablation(args, F, TrajectorySolver, base, plans, coords, Fm, R,
-                                    out.get("plain_fp64"), value, ts)
+        out["ablation"] = _ablation(args, F, TrajectorySolver, base, scenes[nsteps + n_e2e], t,
+                                    out.get("plain_fp64"), ts)
+        out["ablation"]["pose"] = nsteps + n_e2e
     if rank == 0 and world == 1 and not args.no_cpu and _left(args) > 60:
         out["cpu_baseline"] = cpu_baseline(scenes[0], _oracle_iters(st, R))
     out["wall_s"] = round(time.perf_counter() - T_START, 1)
@@ -403,24 +404,29 @@ def _plain_leg(args, F, plan, sc, t, R):
     return rec
 
 
-def _ablation(args, F, TS, base, plans, coords, Fm, R, plain, value, ts_main):
-    """Where the speed-up comes from, on the first timed pose (solves/s):
-      plain     per-RHS cold FP64 PCG, FP64 CUDA-core matvec (the plain leg);
-      batched   all R columns in one cold FP64 PCG on the FP64 CUDA-core
-                matvec: 16 iterations timed, scaled to the iterations of the
-                same batched solve on the INT8 matvec (same recurrences);
-      int8      the same batched cold solve on the INT8 tensor-core matvec, timed;
-      warm      + the quadratic-extrapolation start (FP64 factor), timed;
-      mixed     + the FP32 factor (the timed steps' own mode)."""
+def _ablation(args, F, TS, base, sc, t, plain, ts_main):
+    """Where the speed-up comes from, on one fresh pose of the trajectory
+    (the pose after the ones already solved; solves/s):
+      plain     per-RHS cold FP64 PCG, FP64 CUDA-core matvec, FP64 factor
+                (the plain leg, measured on the first pose);
+      batched   all R columns in one cold batched FP64 PCG on the FP64
+                CUDA-core matvec: 16 iterations timed, scaled to the
+                iterations of the same batched solve on the INT8 matvec (the
+                same per-column recurrences);
+      int8      that batched cold solve on the INT8 tensor-core matvec, timed;
+      block     + block PCG (shared Krylov space), cold, timed;
+      warm      + the quadratic-extrapolation start from the three previous
+                steps, timed;
+      mixed     + the FP32 factor: the timed steps' own configuration, timed."""
     import torch
 
-    k = args.warmup
-    x, nx, y = coords[k]
-    rec = {"pose": k}
-    if plain:
-        rec["plain"] = plain["solves_per_s"]
+    R = 6 * len(sc.moving_bodies())
+    plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
+    x, nx, y = t(sc.x), t(sc.nx), t(sc.y)
+    Fd = t(sc.rhs())
+    F64 = Fd.double()
+    rec = {"plain": plain["solves_per_s"] if plain else None}
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    F64 = Fm[k].double()
 
     def timed(fn):
         torch.cuda.synchronize()
@@ -430,14 +436,14 @@ def _ablation(args, F, TS, base, plans, coords, Fm, R, plain, value, ts_main):
         torch.cuda.synchronize()
         return ev0.elapsed_time(ev1), r
 
-    # batched cold FP64 on the INT8 matvec (fully timed)
-    s8 = F.Solver(plans[k], x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64).set_fp64_matvec("int8")
+    opts = dict(tol=1e-8, max_iters=args.max_iters, check_every=8)
+    s8 = F.Solver(plan, x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64).set_fp64_matvec("int8")
     ms_f8, _ = timed(lambda: s8.factor())
-    ms8, (_, st8) = timed(lambda: s8.solve(F64, tol=1e-8, max_iters=args.max_iters, check_every=8))
+    ms8, (_, st8) = timed(lambda: s8.solve(F64, schedule=F.MBC_SCHED_BATCHED, **opts))
+    msb, (_, stb) = timed(lambda: s8.solve(F64, schedule=F.MBC_SCHED_BLOCK, **opts))
     del s8
     it_b = int(st8["iters_max"])
-    # batched cold FP64 on the CUDA cores: a 16-iteration sample
-    s64 = F.Solver(plans[k], x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64)
+    s64 = F.Solver(plan, x=x, nx=nx, y=y, coef=base.coef, precision=F.MBC_F64)
     ms_f64, _ = timed(lambda: s64.factor())
     ms16, _ = timed(lambda: s64.solve(F64, tol=1e-30, max_iters=16, check_every=16))
     del s64
@@ -445,16 +451,15 @@ def _ablation(args, F, TS, base, plans, coords, Fm, R, plain, value, ts_main):
     rec["batched_note"] = f"16 iterations timed ({ms16:.0f} ms), scaled to {it_b} iterations"
     rec["int8"] = round(1000.0 / (ms_f8 + ms8), 6)
     rec["int8_iters_max"] = it_b
-    # warm-started FP64 (FP64 factor) from the timed steps' own history
-    ts = TS(base.coef, mode="fp64", fp64_matvec=args.fp64_matvec, warm="extrapolate", max_iters=args.max_iters,
-            compact=args.compact)
-    ts.history = list(ts_main.history)
-    msw, (_, stw) = timed(lambda: ts.step(plans[k], x, nx, y, Fm[k], keep=False))
-    rec["warm"] = round(1000.0 / msw, 6)
-    rec["warm_iters_max"] = int(stw["iters_max"])
-    rec["mixed"] = round(value, 6)
-    rec["note"] = ("warm uses the history at the end of the timed steps on the first timed pose: it measures "
-                   "the cost of a warm step, not that pose's own iterations")
+    rec["block"] = round(1000.0 / (ms_f8 + msb), 6)
+    rec["block_iters_max"] = int(stb["iters_max"])
+    for name, mode in (("warm", "fp64"), ("mixed", "mixed")):
+        ts = TS(base.coef, mode=mode, fp64_matvec=args.fp64_matvec, warm="extrapolate",
+                max_iters=args.max_iters, compact=args.compact, schedule=args.schedule)
+        ts.history = list(ts_main.history)
+        ms, (_, stw) = timed(lambda: ts.step(plan, x, nx, y, Fd, keep=False))
+        rec[name] = round(1000.0 / ms, 6)
+        rec[name + "_iters_max"] = int(stw["iters_max"])
     return rec
 
 
@@ -504,74 +509,62 @@ def _learned_start(args, base, q, scenes, dev):
     return Learned()
 
 
-# DRAM bytes (read + write) per launch of the tensor-core matvec at N = Nf =
-# 64000, R = 192, from one ncu capture of the K / K^T probe
-TC_TRAFFIC_BYTES = 442e6
-# the same for the FP64 CUDA-core matvec (pk_rows_kernel<double>, 109.5 MB read
-# + 63.2 MB written at R = 192); its traffic is the vector block in and out,
-# so a launch carrying R columns moves about R / 192 of it
-FP64_TRAFFIC_BYTES_R192 = 172.7e6
-
-
 def _matvec_roofline(st, nf, n, R, matvec, fp64_matvec="simt"):
     """Roofline of the dominant kernel of the timed solve, from live CUDA
-    events: the K / K^T matvec pairs, split by precision.  Algorithmic work
-    per launch: nf * n * (20 + 2 R) flops (R = the columns the launch carries:
-    all R for the FP32 recursion, the polished columns for FP64).  The INT8
-    form of the FP64 matvec is rated on its own work instead: 15 digit-plane
-    products, 2 * 15 * nf * n * R integer ops, against twice the measured
-    dense BF16 rate (the nominal INT8 : BF16 ratio), and on its HBM stream,
-    5 bytes of digit planes per matrix entry."""
+    events on the solver's stream: the K / K^T matvec launches, split by
+    precision, each with the columns it carried (the block PCG narrows as
+    columns converge).  Algorithmic work of a launch carrying c columns:
+    nf * n * (20 + 2 c) flops.  The INT8 form of the FP64 matvec is rated on
+    its own two resources: its INT8 tensor work, 15 digit-plane products =
+    2 * 15 * nf * n * c integer ops, against twice the dense BF16 rate (the
+    nominal INT8 : BF16 ratio); and its HBM stream, the 5 bytes of digit
+    planes per matrix entry that every launch reads whatever its width."""
     hbm, bf16, src = _peaks()
     n64, t64 = st.get("n_matvec64", 0), st.get("t_matvec64_ms", 0.0)
+    c64 = st.get("matvec64_columns", 0) or n64 * R
     n32, t32 = st["n_matvec"] - n64, st["t_matvec_ms"] - t64
-    R64 = max(1, int(st.get("n_polished", 0)) or R)
-
-    def one(t, cnt, cols):
-        ms = t / max(1, cnt)
-        ach = float(nf) * n * (20 + 2 * cols) / (ms * 1e-3) / 1e12 if cnt else 0.0
-        return ms, ach
-
-    ms32, a32 = one(t32, n32, R)
-    ms64, a64 = one(t64, n64, R64)
+    ms32 = t32 / max(1, n32)
+    a32 = float(nf) * n * (20 + 2 * R) * n32 / (t32 * 1e-3) / 1e12 if n32 else 0.0
     tc = {"kernel": ("pk_tc_kernel<0|1> (tcgen05 3xTF32, TMEM accumulators)" if matvec != "simt"
                      else "pk_rows_kernel / pk_cols_kernel<float> (SIMT)"),
           "launch_ms": round(ms32, 3), "launches": int(n32), "achieved_tflops": round(a32, 2),
-          "frac_of_bf16": round(a32 / bf16, 4), "total_ms": round(t32, 1),
-          "traffic": TC_TRAFFIC_BYTES if matvec != "simt" else None}
-    fp64 = {"kernel": "pk_rows_kernel / pk_cols_kernel<double> (FP64 SIMT)", "launch_ms": round(ms64, 3),
-            "launches": int(n64), "columns": R64, "achieved_tflops": round(a64, 2), "total_ms": round(t64, 1),
-            "fp64_nominal_tflops": 37.0, "frac_of_fp64_nominal": round(a64 / 37.0, 4)}
-    dom64 = t64 >= t32
-    if fp64_matvec == "int8":
-        # per launch (one direction): pack + MMA kernel
-        sec = ms64 * 1e-3 if n64 else float("inf")
-        tops = 2.0 * 15 * nf * n * R64 / sec / 1e12
-        gbs = 5.0 * nf * n / sec / 1e9
-        fp64.update({"kernel": "oz_pack_b_kernel + oz_mma_kernel (tcgen05 kind::i8, 5-digit slicing)",
+          "frac_of_bf16": round(a32 / bf16, 4), "total_ms": round(t32, 1)}
+    sec64 = t64 * 1e-3
+    ms64 = t64 / max(1, n64)
+    cols_avg = c64 / max(1, n64)
+    a64 = float(nf) * n * (20.0 * n64 + 2.0 * c64) / sec64 / 1e12 if n64 else 0.0
+    fp64 = {"launch_ms": round(ms64, 3), "launches": int(n64), "columns_per_launch": round(cols_avg, 1),
+            "achieved_tflops_algorithmic": round(a64, 2), "total_ms": round(t64, 1)}
+    if fp64_matvec == "int8" and n64:
+        tops = 2.0 * 15 * nf * n * c64 / sec64 / 1e12
+        gbs = 5.0 * nf * n * n64 / sec64 / 1e9
+        fp64.update({"kernel": "oz_gather + oz_pack_b_kernel + oz_mma_kernel (tcgen05 kind::i8, 5-digit slicing)",
                      "achieved_int8_tops": round(tops, 1), "int8_peak_tops": 2 * bf16,
                      "frac_of_int8": round(tops / (2 * bf16), 4), "plane_gbs": round(gbs, 1),
                      "frac_of_hbm": round(gbs / hbm, 4)})
-        if dom64:
-            tensor_side = tops / (2 * bf16) >= gbs / hbm
-            return {"bound": "tensor" if tensor_side else "hbm",
-                    "achieved": round(tops if tensor_side else gbs, 2),
-                    "peak": 2 * bf16 if tensor_side else hbm, "unit": "TOPS" if tensor_side else "GB/s",
-                    "frac": round(tops / (2 * bf16) if tensor_side else gbs / hbm, 4), "traffic": None,
-                    "kernel": fp64["kernel"], "launch_ms": round(ms64, 3),
-                    "peak_source": f"INT8 dense = 2 x bf16 dense, {src} (derived from measured); "
-                                   f"HBM {hbm} GB/s (of measured)",
-                    "fp64_matvec": fp64, "tensor_matvec": tc}
+        tensor_side = tops / (2 * bf16) >= gbs / hbm
+        return {"bound": "tensor" if tensor_side else "hbm",
+                "achieved": round(tops if tensor_side else gbs, 2),
+                "peak": 2 * bf16 if tensor_side else hbm, "unit": "TOPS" if tensor_side else "GB/s",
+                "frac": round(tops / (2 * bf16) if tensor_side else gbs / hbm, 4), "traffic": OZ_TRAFFIC,
+                "kernel": fp64["kernel"], "launch_ms": round(ms64, 3),
+                "peak_source": f"INT8 dense = 2 x bf16 dense ({src}); HBM {hbm} GB/s ({src})",
+                "fp64_matvec": fp64, "tensor_matvec": tc}
+    fp64.update({"kernel": "pk_rows_kernel / pk_cols_kernel<double> (FP64 SIMT)", "fp64_nominal_tflops": 37.0,
+                 "frac_of_fp64_nominal": round(a64 / 37.0, 4)})
+    dom64 = t64 >= t32
     ach, ms = (a64, ms64) if dom64 else (a32, ms32)
-    if fp64_matvec != "int8" and nf == n == 64000:
-        fp64["traffic"] = round(FP64_TRAFFIC_BYTES_R192 * R64 / 192)
-        fp64["traffic_source"] = "ncu capture at R = 192 (profiles/pk_fp64_matvec_ellipsoids32.md), scaled by columns"
     return {"bound": "tensor", "achieved": round(ach, 2), "peak": bf16, "unit": "TFLOP/s",
-            "frac": round(ach / bf16, 4), "traffic": fp64.get("traffic") if dom64 else tc["traffic"],
+            "frac": round(ach / bf16, 4), "traffic": None,
             "kernel": fp64["kernel"] if dom64 else tc["kernel"], "launch_ms": round(ms, 3),
-            "peak_source": f"bf16 dense, {src} (of measured); the FP64 kernel's own ceiling is the "
-                           f"FP64 pipe (37 TFLOP/s nominal, no measured figure)",
+            "peak_source": f"bf16 dense ({src}); the FP64 kernel's own ceiling is the FP64 pipe "
+                           f"(37 TFLOP/s nominal, no measured figure)",
             "fp64_matvec": fp64, "tensor_matvec": tc}
+
+
+# DRAM bytes (read + write) per launch of the INT8 matvec's MMA kernel, from
+# an ncu capture (filled in from the committed profile summary; None until then)
+OZ_TRAFFIC = None
 
 
 def run_rows(args):
@@ -1081,7 +1074,7 @@ def main():
     ap.add_argument("--reserve-s", type=float, default=420.0,
                     help="seconds kept for the legs after the timed steps (e2e, plain FP64, ablation, CPU)")
     ap.add_argument("--scenes", type=int, default=8, help="uneven workload: scenes in the sample")
-    ap.add_argument("--solver", default="mixed", choices=["mixed", "flexible", "fp64", "mixed64"],
+    ap.add_argument("--solver", default="mixed64", choices=["mixed", "flexible", "fp64", "mixed64"],
                     help="trajectory and uneven: residual-replacement mixed PCG, FP64 flexible CG around the "
                          "FP32 PCG (trajectory), or FP64 PCG (pair with --fp64-matvec int8)")
     ap.add_argument("--inner-iters", type=int, default=40, help="flexible solver: FP32 iterations per outer step")
@@ -1106,7 +1099,7 @@ def main():
     ap.add_argument("--rows-probe", action="store_true",
                     help="time the adjoint solve, the op bodies' cache, the added mass and the mesh assembly "
                          "(one JSON line each)")
-    ap.add_argument("--fp64-matvec", default="simt", choices=["simt", "int8"],
+    ap.add_argument("--fp64-matvec", default="int8", choices=["simt", "int8"],
                     help="FP64 matvec: CUDA-core FP64 kernels or exact INT8 digit slicing on the tensor cores")
     args = ap.parse_args()
     if args.rows_probe:

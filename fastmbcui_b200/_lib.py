@@ -54,7 +54,8 @@ class SolveStats(C.Structure):
                 ("n_converged", C.c_int32), ("relres_max", C.c_double),
                 ("true_relres_max", C.c_double), ("t_solve_ms", C.c_double),
                 ("t_matvec_ms", C.c_double), ("n_matvec", C.c_int64), ("kernel_launches", C.c_int64),
-                ("n_polished", C.c_int32), ("t_matvec64_ms", C.c_double), ("n_matvec64", C.c_int64)]
+                ("n_polished", C.c_int32), ("t_matvec64_ms", C.c_double), ("n_matvec64", C.c_int64),
+                ("matvec64_columns", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

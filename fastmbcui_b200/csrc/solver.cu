@@ -690,6 +690,7 @@ static mbc_status run_pcg(Solver &S, int R, PcgWork<T> &w, XT *x, const LT *lval
         MBC_CK(cudaEventElapsedTime(&ms, S.events[2 * k], S.events[2 * k + 1]));
         S.prof_ms_all.push_back(ms);
         S.prof_is64.push_back(sizeof(T) == 8 ? 1 : 0);
+        S.prof_cols.push_back(cR);
       }
     }
     if (h_flags[0]) break;
@@ -925,6 +926,7 @@ static mbc_status run_block_pcg(Solver &S, int R, PcgWork<double> &w, const LT *
       MBC_CK(cudaEventElapsedTime(&ms, S.events[0], S.events[1]));
       S.prof_ms_all.push_back(ms);
       S.prof_is64.push_back(1);
+      S.prof_cols.push_back(k);
     }
     if (h_small[1]) {  // P^T A P not positive definite (NaN or breakdown): nothing was updated
       failed = true;
@@ -1147,9 +1149,9 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
   const bool compact = o.compact != 0;
   // block PCG (FP64 recursions only; the preconditioner is always applied)
   const bool block = sizeof(T) == 8 && o.schedule == MBC_SCHED_BLOCK && R > 1;
-  // The INT8 operator's recomputed residual can read up to ~10 % below the
-  // FP64 one near tol (measured at N = 64000), so its columns are run and
-  // decided against 0.85 tol.
+  // With the INT8 operator the recursion's own residual drifts from the
+  // FP64 one by up to ~20 % near tol (measured at N = 64000): its columns run
+  // to 0.85 tol, so that few fail the FP64 decision below and restart.
   const double rtol = oz ? 0.85 * o.tol : o.tol;
   if (block) {
     if constexpr (sizeof(T) == 8) {
@@ -1183,21 +1185,35 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
       // accurate residual; replacing the residual inside the recursion
       // instead stalls the ill-conditioned columns (measured: 544 against 179
       // iterations on one column of a 3000-point scene).
+      // The decision residual is FP64-accurate: the products whose inputs
+      // cancel against the right-hand side (K x for the forward residual
+      // f - K x, both products of the adjoint's b - K^T K x) run on the FP64
+      // CUDA-core kernels.  K x of the solution carries the INT8 operator's
+      // ~1e-9 relative error against a least-squares residual f - K x ~1e-7
+      // |f|; K^T of that residual on the INT8 matvec agrees with FP64 to
+      // ~10 digits (measured), so it stays there.  Only |b| (a norm) uses
+      // the solver's FP64 matvec as it is.
       T *bvec = w.Tt;
       if (adjoint) MBC_CK(cudaMemcpyAsync(bvec, fm.ptr, sizeof(T) * nv, cudaMemcpyDeviceToDevice, st));
       else launch_cols<T>(*this, R, (const T *)fm.ptr, bvec, nullptr, nullptr, nullptr, st);
       MBC_CKL();
       std::vector<double> nb;
       MBC_TRY(col_norms2<T>(*this, R, bvec, nb, st));
+      const int32_t impl = fp64_matvec;
       for (int pass = 0; pass < 3; ++pass) {
+        fp64_matvec = MBC_FP64_MATVEC_SIMT;
+        launch_rows<T>(*this, R, w.X, w.W, nullptr, st);
         if (adjoint) {
-          launch_rows<T>(*this, R, w.X, w.W, nullptr, st);
           launch_cols<T>(*this, R, w.W, w.Z, nullptr, nullptr, nullptr, st);
           sub_kernel<T><<<cdiv(nv, 256), 256, 0, st>>>(nv, (const T *)fm.ptr, w.Z, w.Rv);
-          ++launches;
+          fp64_matvec = impl;
         } else {
-          residual<T>(*this, R, (const T *)fm.ptr, w.X, w.W, w.Rv, st);
+          fp64_matvec = impl;
+          const int64_t cnt = (int64_t)nf * R;
+          sub_kernel<T><<<cdiv(cnt, 256), 256, 0, st>>>(cnt, (const T *)fm.ptr, w.W, w.W);
+          launch_cols<T>(*this, R, w.W, w.Rv, nullptr, nullptr, nullptr, st);
         }
+        ++launches;
         MBC_CKL();
         std::vector<double> nr;
         MBC_TRY(col_norms2<T>(*this, R, w.Rv, nr, st));
@@ -1205,7 +1221,7 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
         for (int c = 0; c < R; ++c) {
           rel[c] = nb[c] < 1e-16 ? 0.0 : std::sqrt(nr[c] / nb[c]);
           if (status[c] == COL_BREAKDOWN) continue;
-          status[c] = rel[c] <= rtol ? COL_OK : COL_MAXIT;
+          status[c] = rel[c] <= o.tol ? COL_OK : COL_MAXIT;
           if (status[c] == COL_MAXIT) pol.push_back(c);
         }
         if (pol.empty() || pass == 2) break;
@@ -1448,6 +1464,7 @@ mbc_status Solver::solve(int R, const void *rhs, int32_t rhs_dt, void *X, int32_
   graph = o.graph != 0;
   prof_ms_all.clear();
   prof_is64.clear();
+  prof_cols.clear();
   mbc_status rs;
   if (o.schedule == MBC_SCHED_PER_RHS && R > 1) {
     // one cold-started PCG per column, in order (mfs_torch_ops.cu:166-171)
@@ -1507,6 +1524,7 @@ mbc_status Solver::solve(int R, const void *rhs, int32_t rhs_dt, void *X, int32_
     stats->n_matvec = 0;
     stats->t_matvec64_ms = 0;
     stats->n_matvec64 = 0;
+    stats->matvec64_columns = 0;
     if (profile) {
       // a matvec pair whose kernels exited on the done flag takes a few
       // microseconds; count only pairs that did work (> 1% of the longest of
@@ -1521,6 +1539,7 @@ mbc_status Solver::solve(int R, const void *rhs, int32_t rhs_dt, void *X, int32_
           if (p64) {
             stats->t_matvec64_ms += prof_ms_all[i];
             stats->n_matvec64 += 2;
+            stats->matvec64_columns += 2 * (int64_t)prof_cols[i];
           }
         }
       }

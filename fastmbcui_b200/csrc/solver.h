@@ -42,6 +42,7 @@ struct Solver {
   std::vector<cudaEvent_t> events;
   std::vector<float> prof_ms_all;
   std::vector<int> prof_is64;  // 1: the pair ran in FP64
+  std::vector<int> prof_cols;  // columns the pair carried
 
   // plan on the device
   DevMem m_P, m_Pinv, m_sup_ptr, m_sup_ind, m_set_ptr, m_set_ind, m_lptr, m_lind, m_rptr, m_rcol,

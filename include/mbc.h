@@ -225,6 +225,7 @@ typedef struct {
                                recursion stagnated or ran out of iterations */
   double t_matvec64_ms;     /* profile: the FP64 part of t_matvec_ms */
   int64_t n_matvec64;       /* profile: FP64 K / K^T launches timed */
+  int64_t matvec64_columns; /* profile: columns summed over those launches (block PCG narrows) */
 } mbc_solve_stats;
 
 void mbc_solve_default_options(mbc_solve_options *opt);
