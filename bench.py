@@ -238,6 +238,15 @@ def run_trajectory(args):
         if k == 0:
             cold = st
     torch.cuda.synchronize()
+    if args.profile_step:
+        # one step between profiler start and stop: the launch list of a step
+        k = args.warmup
+        torch.cuda.profiler.start()
+        _, st = ts.step(plans[k], *coords[k], Fm[k], profile=1)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile_step": k, "stats": st}), flush=True)
+        return
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     times, stats = [], []
     # the wall-clock budget: the timed steps stop early (steps_run < steps)
@@ -1083,6 +1092,9 @@ def main():
     ap.add_argument("--warm", default="extrapolate", choices=["extrapolate", "learned", "previous", "cold"],
                     help="trajectory warm start")
     ap.add_argument("--warm-model", default=os.path.join(ROOT, "fastmbcui_b200", "data", "warmstart_mlp.npz"))
+    ap.add_argument("--profile-step", action="store_true",
+                    help="trajectory: only the warm-up steps and one step inside cudaProfilerStart/Stop "
+                         "(for ncu --profile-from-start off); prints the step's stats")
     ap.add_argument("--kernel-probe", action="store_true",
                     help="only run a factor and a few K / K^T launches (ncu captures)")
     ap.add_argument("--probe-reps", type=int, default=3)
