@@ -3,7 +3,7 @@
 The 32-ellipsoid trajectory scene (32 ellipsoids x 2000 points, N = Nf =
 64000, R = 192 rigid-mode columns, rho 3, lambda 1.5, trajectory seed 4) is
 solved by TrajectorySolver exactly as bench.py times it: per step a new host
-plan and factor, all 192 columns in one batched PCG, warm-started by the
+plan and factor, all 192 columns in one block PCG, warm-started by the
 quadratic extrapolation of the previous three steps.  Steps 0-2 build the
 history; step 3 is checked.
 
