@@ -555,7 +555,9 @@ def _matvec_roofline(st, nf, n, R, matvec, fp64_matvec="simt"):
         return {"bound": "tensor" if tensor_side else "hbm",
                 "achieved": round(tops if tensor_side else gbs, 2),
                 "peak": 2 * bf16 if tensor_side else hbm, "unit": "TOPS" if tensor_side else "GB/s",
-                "frac": round(tops / (2 * bf16) if tensor_side else gbs / hbm, 4), "traffic": OZ_TRAFFIC,
+                "frac": round(tops / (2 * bf16) if tensor_side else gbs / hbm, 4),
+                "traffic": round(OZ_TRAFFIC_PER_ENTRY * nf * n),
+                "traffic_source": "ncu at N = Nf = 16000, scaled by the matrix entries",
                 "kernel": fp64["kernel"], "launch_ms": round(ms64, 3),
                 "peak_source": f"INT8 dense = 2 x bf16 dense ({src}); HBM {hbm} GB/s ({src})",
                 "fp64_matvec": fp64, "tensor_matvec": tc}
@@ -571,9 +573,11 @@ def _matvec_roofline(st, nf, n, R, matvec, fp64_matvec="simt"):
             "fp64_matvec": fp64, "tensor_matvec": tc}
 
 
-# DRAM bytes (read + write) per launch of the INT8 matvec's MMA kernel, from
-# an ncu capture (filled in from the committed profile summary; None until then)
-OZ_TRAFFIC = None
+# DRAM bytes (read + write) per matrix entry of one launch of the INT8
+# matvec's MMA kernel: ncu on N = Nf = 16000, R = 48 read 1.2846 GB and wrote
+# 4.1 MB per launch (profiles/oz_mma_kernel_ellipsoids8.md); the planes, and
+# so the traffic, scale with the entries
+OZ_TRAFFIC_PER_ENTRY = (1.2846e9 + 4.1e6) / 16000.0 ** 2
 
 
 def run_rows(args):
