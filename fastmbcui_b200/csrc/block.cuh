@@ -144,16 +144,37 @@ __global__ void __launch_bounds__(kThreads) block_update_kernel(int n, int k, in
 }
 
 // ---------------------------------------------------------------------------
-// Small dense kernels: one block of kSmallThreads threads, matrices in global
-// memory (they stay in L1 / L2).
+// Small dense kernels: one block of kSmallThreads threads.  With use_smem (the
+// caller passes k * k doubles of dynamic shared memory, k <= kSmemDim) the
+// k x k matrix is staged in shared memory, otherwise it stays in global
+// memory (L1 / L2); the arithmetic and its order are the same either way.
+constexpr int kSmemDim = 152;  // 152^2 doubles = 180.5 KB
+
+__device__ __forceinline__ void stage_in(int k, const double *src, int ld, double *dst)
+{
+  for (int64_t t = threadIdx.x; t < (int64_t)k * k; t += blockDim.x) {
+    const int i = (int)(t / k), j = (int)(t % k);
+    dst[t] = src[(size_t)i * ld + j];
+  }
+  __syncthreads();
+}
 
 // In place lower Cholesky of the k x k SPD matrix G (row-major, ld):
 // G = L L^T, L in the lower triangle (the strict upper triangle is left as
 // is).  *flag = 1 on a pivot that is not positive (or NaN).
-__global__ void __launch_bounds__(kSmallThreads) chol_kernel(int k, double *G, int ld, int32_t *flag)
+__global__ void __launch_bounds__(kSmallThreads) chol_kernel(int k, double *Gg, int ldg, int32_t *flag,
+                                                             int use_smem)
 {
+  extern __shared__ double sm[];
   __shared__ int bad;
   if (threadIdx.x == 0) bad = 0;
+  double *G = Gg;
+  int ld = ldg;
+  if (use_smem) {
+    stage_in(k, Gg, ldg, sm);
+    G = sm;
+    ld = k;
+  }
   __syncthreads();
   for (int j = 0; j < k; ++j) {
     if (threadIdx.x == 0) {
@@ -173,16 +194,29 @@ __global__ void __launch_bounds__(kSmallThreads) chol_kernel(int k, double *G, i
     }
     __syncthreads();
   }
+  if (use_smem)
+    for (int64_t t = threadIdx.x; t < (int64_t)k * k; t += blockDim.x) {
+      const int i = (int)(t / k), j = (int)(t % k);
+      if (j <= i) Gg[(size_t)i * ldg + j] = sm[t];
+    }
   if (threadIdx.x == 0 && bad && flag) *flag = 1;
 }
 
 // B (k x m, ldb) <- sgn * (L L^T)^{-1} B, L lower from chol_kernel; nothing
 // is done when *skip is set (the factorization failed)
-__global__ void __launch_bounds__(kSmallThreads) chol_solve_kernel(int k, const double *L, int ld, int m,
+__global__ void __launch_bounds__(kSmallThreads) chol_solve_kernel(int k, const double *Lg, int ldg, int m,
                                                                    double *B, int ldb, double sgn,
-                                                                   const int32_t *skip)
+                                                                   const int32_t *skip, int use_smem)
 {
+  extern __shared__ double sm[];
   if (skip && *skip) return;
+  const double *L = Lg;
+  int ld = ldg;
+  if (use_smem) {
+    stage_in(k, Lg, ldg, sm);
+    L = sm;
+    ld = k;
+  }
   // forward: L y = b
   for (int j = 0; j < k; ++j) {
     const double ljj = L[(size_t)j * ld + j];
@@ -224,10 +258,18 @@ constexpr int kOrthMax = 512;  // widest block orth_factor_kernel takes
 // columns used) such that V T[:, :r] has orthonormal columns in exact
 // arithmetic: T = D Pi U^{-1}, D the column scaling, Pi^T D W D Pi = U^T U on
 // the kept pivots; and *rank = r.  Work: perm[m] int32.
-__global__ void __launch_bounds__(kSmallThreads) orth_factor_kernel(int m, double *W, int ld, double drop,
+__global__ void __launch_bounds__(kSmallThreads) orth_factor_kernel(int m, double *Wg, int ldg, double drop,
                                                                     double *T, int ldt, int32_t *perm,
-                                                                    int32_t *rank)
+                                                                    int32_t *rank, int use_smem)
 {
+  extern __shared__ double sm[];
+  double *W = Wg;
+  int ld = ldg;
+  if (use_smem) {
+    stage_in(m, Wg, ldg, sm);
+    W = sm;
+    ld = m;
+  }
   __shared__ double s_val[32];
   __shared__ int s_idx[32];
   __shared__ int s_r;

@@ -800,6 +800,10 @@ __global__ void block_fail_kernel(int a, const int32_t *__restrict__ act, PcgSca
 // w.X holds x0 and w.Rv the residual b - A x0 (new order, n x R); on exit
 // w.X holds the solutions and w.sc the per-column status, iterations and
 // |r|^2.  FP64 throughout (the matvec per the solver's FP64 choice).
+// columns the block PCG keeps while any column iterates (the INT8 matvec's
+// narrowest column group)
+constexpr int kBlockKeep = 16;
+
 template <typename LT>
 static mbc_status run_block_pcg(Solver &S, int R, PcgWork<double> &w, const LT *lval, int maxit, double tol,
                                 const double *d_b2ref, cudaStream_t st)
@@ -851,32 +855,28 @@ static mbc_status run_block_pcg(Solver &S, int R, PcgWork<double> &w, const LT *
                                                                       U, Zm, Rm, w.part, nullptr);
     S.launches += 2;
   };
+  // the small factorizations run in shared memory when their matrix fits
+  const size_t smem_max = sizeof(double) * blk::kSmemDim * blk::kSmemDim;
+  MBC_TRY(allow_max_smem(blk::chol_kernel, smem_max));
+  MBC_TRY(allow_max_smem(blk::chol_solve_kernel, smem_max));
+  MBC_TRY(allow_max_smem(blk::orth_factor_kernel, smem_max));
+  auto smem_of = [](int k) -> size_t { return k <= blk::kSmemDim ? sizeof(double) * k * k : 0; };
   // P (n x r, ld r) = an orthonormal basis of the columns of Vin (n x m, ld
   // m; Vin is P's partner buffer V or Z, not needed afterwards), dependent
-  // directions dropped; r = 0 when none is left.  Pass 1 writes P, pass 2 V,
-  // then P and V swap.
+  // directions dropped; r = 0 when none is left.  One Cholesky QR pass: the
+  // drop bounds the kept block's condition by ~1e6, so P's orthogonality
+  // error, of order eps cond^2 <= 1e-4, leaves P^T A P well conditioned,
+  // which is all the recursion needs (it never assumes P^T P = I).
   auto orth = [&](const double *Vin, int m, int *r_out) -> mbc_status {
     gram(Vin, m, m, Vin, m, m, Wm);
-    blk::orth_factor_kernel<<<1, blk::kSmallThreads, 0, st>>>(m, Wm, R, 1e-6, T1, R, d_perm, d_small);
+    blk::orth_factor_kernel<<<1, blk::kSmallThreads, smem_of(m), st>>>(m, Wm, R, 1e-6, T1, R, d_perm, d_small,
+                                                                        m <= blk::kSmemDim);
     MBC_CK(cudaMemcpyAsync(h_small, d_small, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     MBC_CK(cudaStreamSynchronize(st));
     const int r = h_small[0];
     ++S.launches;
     *r_out = r;
-    if (r == 0) return MBC_OK;
-    update(m, r, Vin, m, T1, nullptr, 0, 1.0, P, r);
-    // second pass: the first leaves an orthogonality error of order
-    // eps cond^2, which the second removes (cond <= 1e6 after the drop)
-    gram(P, r, r, P, r, r, Wm);
-    blk::orth_factor_kernel<<<1, blk::kSmallThreads, 0, st>>>(r, Wm, R, 0.0, T2, R, d_perm, d_small);
-    MBC_CK(cudaMemcpyAsync(h_small, d_small, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    MBC_CK(cudaStreamSynchronize(st));
-    const int r2 = h_small[0];
-    ++S.launches;
-    *r_out = r2;
-    if (r2 == 0) return MBC_OK;
-    update(r, r2, P, r, T2, nullptr, 0, 1.0, V, r2);
-    std::swap(P, V);
+    if (r > 0) update(m, r, Vin, m, T1, nullptr, 0, 1.0, P, r);
     return MBC_OK;
   };
   // the active columns, gathered into the compact block
@@ -906,8 +906,9 @@ static mbc_status run_block_pcg(Solver &S, int R, PcgWork<double> &w, const LT *
     gram(P, k, k, Q, k, k, G);
     gram(P, k, k, Ra[cur], a, a, Sm);
     MBC_CK(cudaMemsetAsync(d_flag, 0, sizeof(int32_t), st));
-    blk::chol_kernel<<<1, blk::kSmallThreads, 0, st>>>(k, G, R, d_flag);
-    blk::chol_solve_kernel<<<1, blk::kSmallThreads, 0, st>>>(k, G, R, a, Sm, R, 1.0, d_flag);
+    blk::chol_kernel<<<1, blk::kSmallThreads, smem_of(k), st>>>(k, G, R, d_flag, k <= blk::kSmemDim);
+    blk::chol_solve_kernel<<<1, blk::kSmallThreads, smem_of(k), st>>>(k, G, R, a, Sm, R, 1.0, d_flag,
+                                                                       k <= blk::kSmemDim);
     update(k, a, P, k, Sm, Xa[cur], a, 1.0, Xa[cur], a, d_flag);
     update(k, a, Q, k, Sm, Ra[cur], a, -1.0, Ra[cur], a, d_flag);
     // per-column stop test on |r|^2
@@ -935,7 +936,20 @@ static mbc_status run_block_pcg(Solver &S, int R, PcgWork<double> &w, const LT *
     std::vector<int32_t> keep;  // positions in the compact block of the columns still active
     for (int j = 0; j < a; ++j)
       if (status[act[j]] == COL_ACTIVE) keep.push_back(j);
-    const int a2 = (int)keep.size();
+    const int nact = (int)keep.size();
+    // While any column iterates, the block keeps at least kBlockKeep columns:
+    // converged ones stay in (their x keeps improving; their stop state is
+    // final) and go on feeding the shared Krylov space with directions, at
+    // no matvec cost, since the INT8 matvec's work does not shrink below 16
+    // columns.  The slowest columns' tail is where this pays.
+    if (nact > 0 && nact < std::min(a, kBlockKeep)) {
+      std::vector<char> in(a, 0);
+      for (int j : keep) in[j] = 1;
+      for (int j = a - 1; j >= 0 && (int)keep.size() < std::min(a, kBlockKeep); --j)
+        if (!in[j]) keep.push_back(j);
+      std::sort(keep.begin(), keep.end());
+    }
+    const int a2 = nact == 0 ? 0 : (int)keep.size();
     if (a2 < a) {
       // finished columns' x back to the batch (the others are rewritten later)
       scatter_cols_kernel<double><<<cdiv((int64_t)n * a, 256), 256, 0, st>>>(n, R, a, d_act, Xa[cur], w.X);
@@ -958,7 +972,8 @@ static mbc_status run_block_pcg(Solver &S, int R, PcgWork<double> &w, const LT *
     // next search block: P = orth(Z + P beta), beta = -(P^T A P)^-1 Q^T Z
     precond(a, Ra[cur], Z);
     gram(Q, k, k, Z, a, a, H);
-    blk::chol_solve_kernel<<<1, blk::kSmallThreads, 0, st>>>(k, G, R, a, H, R, -1.0, nullptr);
+    blk::chol_solve_kernel<<<1, blk::kSmallThreads, smem_of(k), st>>>(k, G, R, a, H, R, -1.0, nullptr,
+                                                                       k <= blk::kSmemDim);
     update(k, a, P, k, H, Z, a, 1.0, V, a);
     S.launches += 1;
     MBC_TRY(orth(V, a, &k));
@@ -1200,37 +1215,45 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
       std::vector<double> nb;
       MBC_TRY(col_norms2<T>(*this, R, bvec, nb, st));
       const int32_t impl = fp64_matvec;
-      for (int pass = 0; pass < 3; ++pass) {
+      // the decision residual of Rc columns: F (rhs, nf x Rc; adjoint: b,
+      // n x Rc), X (n x Rc) -> Rout (n x Rc), with Wc (nf x Rc), Zc (n x Rc)
+      auto resid = [&](int Rc, const T *Fc, const T *Xc, T *Wc, T *Zc, T *Rout) {
         fp64_matvec = MBC_FP64_MATVEC_SIMT;
-        launch_rows<T>(*this, R, w.X, w.W, nullptr, st);
+        launch_rows<T>(*this, Rc, Xc, Wc, nullptr, st);
         if (adjoint) {
-          launch_cols<T>(*this, R, w.W, w.Z, nullptr, nullptr, nullptr, st);
-          sub_kernel<T><<<cdiv(nv, 256), 256, 0, st>>>(nv, (const T *)fm.ptr, w.Z, w.Rv);
+          launch_cols<T>(*this, Rc, Wc, Zc, nullptr, nullptr, nullptr, st);
+          const int64_t cnt = (int64_t)n * Rc;
+          sub_kernel<T><<<cdiv(cnt, 256), 256, 0, st>>>(cnt, Fc, Zc, Rout);
           fp64_matvec = impl;
         } else {
           fp64_matvec = impl;
-          const int64_t cnt = (int64_t)nf * R;
-          sub_kernel<T><<<cdiv(cnt, 256), 256, 0, st>>>(cnt, (const T *)fm.ptr, w.W, w.W);
-          launch_cols<T>(*this, R, w.W, w.Rv, nullptr, nullptr, nullptr, st);
+          const int64_t cnt = (int64_t)nf * Rc;
+          sub_kernel<T><<<cdiv(cnt, 256), 256, 0, st>>>(cnt, Fc, Wc, Wc);
+          launch_cols<T>(*this, Rc, Wc, Rout, nullptr, nullptr, nullptr, st);
         }
         ++launches;
-        MBC_CKL();
-        std::vector<double> nr;
-        MBC_TRY(col_norms2<T>(*this, R, w.Rv, nr, st));
-        std::vector<int32_t> pol;
-        for (int c = 0; c < R; ++c) {
-          rel[c] = nb[c] < 1e-16 ? 0.0 : std::sqrt(nr[c] / nb[c]);
-          if (status[c] == COL_BREAKDOWN) continue;
-          status[c] = rel[c] <= o.tol ? COL_OK : COL_MAXIT;
-          if (status[c] == COL_MAXIT) pol.push_back(c);
-        }
-        if (pol.empty() || pass == 2) break;
+      };
+      // every column decided once; the restarted ones then re-decided alone
+      resid(R, (const T *)fm.ptr, w.X, w.W, w.Z, w.Rv);
+      MBC_CKL();
+      std::vector<double> nr;
+      MBC_TRY(col_norms2<T>(*this, R, w.Rv, nr, st));
+      std::vector<int32_t> pol;
+      for (int c = 0; c < R; ++c) {
+        rel[c] = nb[c] < 1e-16 ? 0.0 : std::sqrt(nr[c] / nb[c]);
+        if (status[c] == COL_BREAKDOWN) continue;
+        status[c] = rel[c] <= o.tol ? COL_OK : COL_MAXIT;
+        if (status[c] == COL_MAXIT) pol.push_back(c);
+      }
+      const int frows = adjoint ? n : nf;
+      for (int pass = 0; pass < 2 && !pol.empty(); ++pass) {
         const int Rs = (int)pol.size();
         PcgWork<T> ws;
-        DevMem wmem, wpart, wscal, widx;
+        DevMem wmem, wpart, wscal, widx, fsub;
         MBC_TRY(pcg_buffers_in<T>(*this, Rs, ws, wmem, wpart, wscal));
         const size_t ib = ((sizeof(int32_t) * Rs) + 15) & ~(size_t)15;
         MBC_TRY(widx.reserve(ib + sizeof(double) * Rs));
+        MBC_TRY(fsub.reserve(sizeof(T) * (size_t)frows * Rs));
         int32_t *d_idx = (int32_t *)widx.ptr;
         double *d_b2s = (double *)((char *)widx.ptr + ib);
         std::vector<double> b2s(Rs);
@@ -1240,7 +1263,9 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
         const int64_t ns = (int64_t)n * Rs;
         gather_cols_kernel<T><<<cdiv(ns, 256), 256, 0, st>>>(n, R, Rs, d_idx, w.X, ws.X);
         gather_cols_kernel<T><<<cdiv(ns, 256), 256, 0, st>>>(n, R, Rs, d_idx, w.Rv, ws.Rv);
-        launches += 2;
+        gather_cols_kernel<T><<<cdiv((int64_t)frows * Rs, 256), 256, 0, st>>>(frows, R, Rs, d_idx,
+                                                                             (const T *)fm.ptr, (T *)fsub.ptr);
+        launches += 3;
         MBC_CKL();
         if (precision == MBC_F64)
           MBC_TRY((run_pcg<T, double, T>(*this, Rs, ws, ws.X, (const double *)lval.ptr, o.max_iters, rtol,
@@ -1252,11 +1277,23 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
                                         nullptr, 0, compact)));
         std::vector<int32_t> it2(Rs);
         MBC_CK(cudaMemcpyAsync(it2.data(), ws.sc.iters, sizeof(int32_t) * Rs, cudaMemcpyDeviceToHost, st));
+        // the restarted columns' x back, and their own decision residual
         scatter_cols_kernel<T><<<cdiv(ns, 256), 256, 0, st>>>(n, R, Rs, d_idx, ws.X, w.X);
-        ++launches;
+        resid(Rs, (const T *)fsub.ptr, ws.X, ws.W, ws.Z, ws.Rv);
+        scatter_cols_kernel<T><<<cdiv(ns, 256), 256, 0, st>>>(n, R, Rs, d_idx, ws.Rv, w.Rv);
+        launches += 2;
         MBC_CKL();
-        MBC_CK(cudaStreamSynchronize(st));
-        for (int k = 0; k < Rs; ++k) iters[pol[k]] += it2[k];
+        std::vector<double> nrs;
+        MBC_TRY(col_norms2<T>(*this, Rs, ws.Rv, nrs, st));
+        std::vector<int32_t> again;
+        for (int k = 0; k < Rs; ++k) {
+          const int c = pol[k];
+          iters[c] += it2[k];
+          rel[c] = nb[c] < 1e-16 ? 0.0 : std::sqrt(nrs[k] / nb[c]);
+          status[c] = rel[c] <= o.tol ? COL_OK : COL_MAXIT;
+          if (status[c] == COL_MAXIT) again.push_back(c);
+        }
+        pol.swap(again);
       }
     }
   }
