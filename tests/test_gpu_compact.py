@@ -6,12 +6,7 @@ iterations within 2 per column (the per-column dot products are grouped
 differently at another width), fitted flux within 1e-8 of |F|, FP64 true
 residual <= 1.05e-8 per column.  Also with the INT8 FP64 matvec (its
 restarted columns).
-
-Skipped unless MBC_FIRST_GPU_RUN=1: these paths wait for their first
-supervised GPU run.
 """
-import os
-
 import numpy as np
 import pytest
 
@@ -19,9 +14,7 @@ import fastmbcui_b200 as F
 import oracle as O
 from fastmbcui_b200 import scenes as S
 
-pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(os.environ.get("MBC_FIRST_GPU_RUN") != "1",
-                                 reason="first supervised GPU run pending (MBC_FIRST_GPU_RUN=1)")]
+pytestmark = pytest.mark.gpu
 
 torch = pytest.importorskip("torch")
 

@@ -13,12 +13,7 @@ the scheme's worst-case error; kc = 2048-wide chunk length):
     than the FP64 kernels (the operator's ~1e-9 relative product error slows
     the ill-conditioned columns: 264 against 225 on this scene, measured on
     the B200), fitted flux within 1e-6 of theirs (relative to |F|).
-
-The tests that run the INT8 kernels are skipped unless MBC_FIRST_GPU_RUN=1: they
-wait for their first supervised GPU run.
 """
-import os
-
 import numpy as np
 import pytest
 
@@ -28,8 +23,6 @@ from fastmbcui_b200 import _lib
 from fastmbcui_b200 import scenes as S
 
 pytestmark = pytest.mark.gpu
-int8_run = pytest.mark.skipif(os.environ.get("MBC_FIRST_GPU_RUN") != "1",
-                              reason="INT8 matvec kernels: first supervised GPU run pending (MBC_FIRST_GPU_RUN=1)")
 
 torch = pytest.importorskip("torch")
 CHUNK = 2048
@@ -79,7 +72,6 @@ def case():
     return Case()
 
 
-@int8_run
 @pytest.mark.parametrize("R", [1, 12, 100, 192])
 def test_apply_K(case, R):
     sc = case.sc
@@ -94,7 +86,6 @@ def test_apply_K(case, R):
     assert np.linalg.norm(W8 - W64) / np.linalg.norm(W64) <= 1e-9
 
 
-@int8_run
 @pytest.mark.parametrize("R", [1, 12, 192])
 def test_apply_KT(case, R):
     sc = case.sc
@@ -110,7 +101,6 @@ def test_apply_KT(case, R):
     assert np.linalg.norm(T8 - T64) / np.linalg.norm(T64) <= 1e-9
 
 
-@int8_run
 def test_fp64_solve_on_int8_matvec(case):
     sc = case.sc
     op = O.Op.from_scene(sc)
@@ -128,7 +118,6 @@ def test_fp64_solve_on_int8_matvec(case):
     assert np.linalg.norm(op.K(X8) - op.K(X64)) / np.linalg.norm(Fm) < 1e-6
 
 
-@int8_run
 def test_mixed_solve_polishes_on_int8_matvec(case):
     sc = case.sc
     op = O.Op.from_scene(sc)
