@@ -170,6 +170,29 @@ class Solver:
         check(load().mbc_solver_prepare(self._h, self._sp()), "mbc_solver_prepare")
         return self
 
+    def set_factor_tiles(self, tiles: dict):
+        """Factor tile shapes (mbc_solver_set_factor_tiles): {"max_ns": [3],
+        "tile_rows": [4]}."""
+        t = _lib.FactorTiles()
+        t.max_ns[:] = [int(v) for v in tiles["max_ns"]]
+        t.tile_rows[:] = [int(v) for v in tiles["tile_rows"]]
+        check(load().mbc_solver_set_factor_tiles(self._h, C.byref(t)), "mbc_solver_set_factor_tiles")
+        return self
+
+    def factor_tiles(self) -> dict:
+        t = _lib.FactorTiles()
+        check(load().mbc_solver_get_factor_tiles(self._h, C.byref(t)), "mbc_solver_get_factor_tiles")
+        return t.as_dict()
+
+    def tune_factor(self, reps: int = 2):
+        """Autotune the factor's tile shapes on this solver (mbc_solver_tune_factor);
+        returns (tiles, best factor ms).  The solver ends factored with them."""
+        t = _lib.FactorTiles()
+        ms = C.c_double()
+        check(load().mbc_solver_tune_factor(self._h, int(reps), C.byref(t), C.byref(ms), self._sp()),
+              "mbc_solver_tune_factor")
+        return t.as_dict(), ms.value
+
     def pivot_retries(self) -> int:
         c = C.c_int32(0)
         check(load().mbc_solver_get_pivot_retries(self._h, C.byref(c)), "get_pivot_retries")

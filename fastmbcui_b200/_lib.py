@@ -48,6 +48,13 @@ class SolveOptions(C.Structure):
                 ("graph", C.c_int32), ("compact", C.c_int32), ("fp64_recursion", C.c_int32)]
 
 
+class FactorTiles(C.Structure):
+    _fields_ = [("max_ns", C.c_int32 * 3), ("tile_rows", C.c_int32 * 4)]
+
+    def as_dict(self):
+        return {"max_ns": list(self.max_ns), "tile_rows": list(self.tile_rows)}
+
+
 class SolveStats(C.Structure):
     _fields_ = [("status_per_worst", C.c_int32), ("iters_max", C.c_int32),
                 ("iters_total", C.c_int64), ("refinements", C.c_int32),
@@ -76,6 +83,10 @@ SIGNATURES = {
     "mbc_plan_get_supernodes": (C.c_int, [_vp, _vp, _vp, _vp]),
     "mbc_plan_get_factor_pattern": (C.c_int, [_vp, _vp, _vp]),
     "mbc_spatial_order": (C.c_int, [_i32, _vp, _i32, _vp]),
+    "mbc_factor_default_tiles": (None, [C.POINTER(FactorTiles)]),
+    "mbc_solver_set_factor_tiles": (C.c_int, [_vp, C.POINTER(FactorTiles)]),
+    "mbc_solver_get_factor_tiles": (C.c_int, [_vp, C.POINTER(FactorTiles)]),
+    "mbc_solver_tune_factor": (C.c_int, [_vp, _i32, C.POINTER(FactorTiles), C.POINTER(C.c_double), _vp]),
     "mbc_solver_create": (C.c_int, [_vp, C.POINTER(Operator), _i32, _vp, C.POINTER(_vp)]),
     "mbc_solver_destroy": (C.c_int, [_vp]),
     "mbc_solver_factor": (C.c_int, [_vp, _vp]),

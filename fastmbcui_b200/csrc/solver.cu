@@ -243,15 +243,22 @@ template int launch_cols<double>(const Solver &, int, const double *, double *, 
 // --------------------------------------------------------------------------
 namespace {
 
-struct ClassSpec {
-  int max_ns;  // inclusive upper bound of n_s for this class (0 = unbounded)
-  int nt, tile_rows;
-};
 // FP32 supernodes whose pivots cancel below this fraction of their diagonal
 // (more than ~3 of FP32's ~7 digits lost) are refactored in FP64.
 constexpr double kF32PivotTol = 1e-3;
-// n_s <= 32, <= 64, <= 128 in shared memory; larger ones in global memory
-constexpr ClassSpec kClasses[4] = {{32, 128, 64}, {64, 256, 32}, {128, 512, 32}, {0, 512, 8}};
+// threads per class; the class bounds and panel rows come from the solver's
+// mbc_factor_tiles (default: n_s <= 32, <= 64, <= 128 in shared memory,
+// larger ones in global memory; 64, 32, 32, 8 panel rows)
+constexpr int kClassThreads[4] = {128, 256, 512, 512};
+
+// the dynamic shared memory a block may opt in to on this device
+static int smem_optin_cap()
+{
+  int dev = 0, cap = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 48 * 1024;
+  if (cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 48 * 1024;
+  return cap - 1024;  // room for the kernel's static shared variables
+}
 
 template <typename T>
 size_t factor_smem(int ns_max, int nt, int tr, bool theta_in_smem)
@@ -310,18 +317,22 @@ static mbc_status run_factor(Solver &S, const std::vector<int32_t> *lists, T *th
     a.pivot_tol = pivot_tol;
     a.bad_list = d_bad_list;
     a.bad_count = d_bad_count;
-    const ClassSpec cs = kClasses[c];
-    const bool in_smem = cs.max_ns > 0;
-    int tr = cs.tile_rows;
+    const int nt = kClassThreads[c];
+    const bool in_smem = c < 3;
+    int tr = std::max(1, S.tiles.tile_rows[c]);
     if (!in_smem) {
-      tr = (int)std::max<int64_t>(1, std::min<int64_t>(32, (96 * 1024) / ((int64_t)ns_max * sizeof(T))));
-      MBC_TRY(S.fscratch.reserve((size_t)lst.size() * (cs.nt / 32) * ns_max * sizeof(T)));
+      tr = (int)std::max<int64_t>(1, std::min<int64_t>(tr, (96 * 1024) / ((int64_t)ns_max * sizeof(T))));
+      MBC_TRY(S.fscratch.reserve((size_t)lst.size() * (nt / 32) * ns_max * sizeof(T)));
       a.gscratch = S.fscratch.ptr;
       a.gscratch_stride = ns_max;
     }
-    a.smem_cap = in_smem ? cs.max_ns : 0;
+    // fewer panel rows where the class's Theta and buffers leave too little
+    // shared memory (the FP64 retries need twice the FP32 launch's)
+    const size_t cap = (size_t)smem_optin_cap();
+    while (tr > 1 && factor_smem<T>(ns_max, nt, tr, in_smem) > cap) tr /= 2;
+    a.smem_cap = in_smem ? S.tiles.max_ns[c] : 0;
     a.tile_rows = tr;
-    const size_t smem = factor_smem<T>(ns_max, cs.nt, tr, in_smem);
+    const size_t smem = factor_smem<T>(ns_max, nt, tr, in_smem);
     switch (c) {
       case 0: MBC_TRY((launch_factor_class<T, LT, 128, 5>(a, theta, lval, smem, st))); break;
       case 1: MBC_TRY((launch_factor_class<T, LT, 256, 9>(a, theta, lval, smem, st))); break;
@@ -332,14 +343,15 @@ static mbc_status run_factor(Solver &S, const std::vector<int32_t> *lists, T *th
   return MBC_OK;
 }
 
-static void split_classes(const Plan &p, const std::vector<int32_t> &ids, std::vector<int32_t> *lists)
+static void split_classes(const Plan &p, const mbc_factor_tiles &t, const std::vector<int32_t> &ids,
+                          std::vector<int32_t> *lists)
 {
   for (int c = 0; c < 4; ++c) lists[c].clear();
   for (int32_t s : ids) {
     const int ns = p.set_ptr[s + 1] - p.set_ptr[s];
     int c = 3;
     for (int k = 0; k < 3; ++k)
-      if (ns <= kClasses[k].max_ns) {
+      if (ns <= t.max_ns[k]) {
         c = k;
         break;
       }
@@ -367,7 +379,7 @@ mbc_status Solver::factor(cudaStream_t st)
   std::vector<int32_t> all(p.n_super);
   for (int32_t s = 0; s < p.n_super; ++s) all[s] = s;
   std::vector<int32_t> lists[4];
-  split_classes(p, all, lists);
+  split_classes(p, tiles, all, lists);
   if (precision == MBC_F64)
     MBC_TRY((run_factor<double, double>(*this, lists, (double *)theta.ptr, (double *)lval.ptr, 0.0,
                                         0.0, d_bad_list, d_bad_count, st)));
@@ -388,7 +400,7 @@ mbc_status Solver::factor(cudaStream_t st)
     MBC_CK(cudaMemcpy(ids.data(), d_bad_list, sizeof(int32_t) * nbad, cudaMemcpyDeviceToHost));
     pivot_retries += nbad;
     MBC_CK(cudaMemsetAsync(d_bad_count, 0, sizeof(int32_t), st));
-    split_classes(p, ids, lists);
+    split_classes(p, tiles, ids, lists);
     MBC_TRY(theta64.reserve(std::max<size_t>(th_n * 8, 16)));
     if (precision == MBC_F64)
       MBC_TRY((run_factor<double, double>(*this, lists, (double *)theta.ptr, (double *)lval.ptr,
@@ -1673,6 +1685,108 @@ extern "C" mbc_status mbc_solver_factor(mbc_solver *s, mbc_stream stream)
 {
   if (!s) return fail(MBC_BAD_ARG, "NULL solver");
   return s->s.factor((cudaStream_t)stream);
+}
+
+extern "C" void mbc_factor_default_tiles(mbc_factor_tiles *t)
+{
+  if (!t) return;
+  *t = mbc_factor_tiles{{32, 64, 128}, {64, 32, 32, 8}};
+}
+
+static bool tiles_valid(const mbc_factor_tiles &t)
+{
+  if (t.max_ns[0] < 1 || t.max_ns[0] >= t.max_ns[1] || t.max_ns[1] >= t.max_ns[2] || t.max_ns[2] > 144) return false;
+  for (int c = 0; c < 4; ++c)
+    if (t.tile_rows[c] < 1 || t.tile_rows[c] > 256) return false;
+  return true;
+}
+
+extern "C" mbc_status mbc_solver_set_factor_tiles(mbc_solver *s, const mbc_factor_tiles *t)
+{
+  if (!s || !t) return fail(MBC_BAD_ARG, "NULL solver or tiles");
+  if (!tiles_valid(*t)) return fail(MBC_BAD_ARG, "factor tiles: need 1 <= max_ns[0] < max_ns[1] < max_ns[2] <= 144 "
+                                                 "and 1 <= tile_rows <= 256");
+  s->s.tiles = *t;
+  return MBC_OK;
+}
+
+extern "C" mbc_status mbc_solver_get_factor_tiles(const mbc_solver *s, mbc_factor_tiles *t)
+{
+  if (!s || !t) return fail(MBC_BAD_ARG, "NULL solver or tiles");
+  *t = s->s.tiles;
+  return MBC_OK;
+}
+
+extern "C" mbc_status mbc_solver_tune_factor(mbc_solver *s, int32_t reps, mbc_factor_tiles *best_out,
+                                             double *ms_best, mbc_stream stream)
+{
+  if (!s || reps < 1) return fail(MBC_BAD_ARG, "NULL solver or reps < 1");
+  mbc::Solver &S = s->s;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaEvent_t e0, e1;
+  MBC_CK(cudaEventCreate(&e0));
+  MBC_CK(cudaEventCreate(&e1));
+  struct Ev {
+    cudaEvent_t a, b;
+    ~Ev()
+    {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  } ev{e0, e1};
+  // the median of `reps` factor times of a candidate; +inf if it cannot run
+  auto time_of = [&](const mbc_factor_tiles &t) -> double {
+    if (!tiles_valid(t)) return INFINITY;
+    S.tiles = t;
+    std::vector<float> ms;
+    for (int r = 0; r < reps; ++r) {
+      cudaEventRecord(e0, st);
+      if (S.factor(st) != MBC_OK) return INFINITY;
+      cudaEventRecord(e1, st);
+      if (cudaEventSynchronize(e1) != cudaSuccess) return INFINITY;
+      float m = 0.f;
+      cudaEventElapsedTime(&m, e0, e1);
+      ms.push_back(m);
+    }
+    std::sort(ms.begin(), ms.end());
+    return ms[ms.size() / 2];
+  };
+  mbc_factor_tiles best = S.tiles;
+  double tbest = time_of(best);
+  // class bounds, with the current panel rows
+  const int b0s[3] = {24, 32, 48}, b1s[2] = {64, 96}, b2s[2] = {128, 144};
+  for (int b0 : b0s)
+    for (int b1 : b1s)
+      for (int b2 : b2s) {
+        mbc_factor_tiles t = best;
+        t.max_ns[0] = b0;
+        t.max_ns[1] = b1;
+        t.max_ns[2] = b2;
+        const double tm = time_of(t);
+        if (tm < tbest) {
+          tbest = tm;
+          best = t;
+        }
+      }
+  // then the panel rows, one class at a time
+  const int rows[5] = {8, 16, 32, 64, 128};
+  for (int c = 0; c < 4; ++c)
+    for (int r : rows) {
+      mbc_factor_tiles t = best;
+      t.tile_rows[c] = r;
+      const double tm = time_of(t);
+      if (tm < tbest) {
+        tbest = tm;
+        best = t;
+      }
+    }
+  S.tiles = best;
+  MBC_TRY(S.factor(st));
+  MBC_CK(cudaStreamSynchronize(st));
+  if (!std::isfinite(tbest)) return fail(MBC_CUDA_ERROR, "factor tuning: no candidate ran");
+  if (best_out) *best_out = best;
+  if (ms_best) *ms_best = tbest;
+  return MBC_OK;
 }
 
 extern "C" mbc_status mbc_solver_get_factor(const mbc_solver *s, double *lval_host, double *theta_host)

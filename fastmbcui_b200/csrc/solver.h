@@ -35,6 +35,7 @@ struct Solver {
   bool graph = false;  // replay PCG iteration blocks as CUDA graphs
   int32_t matvec_impl = MBC_MATVEC_AUTO;
   int32_t fp64_matvec = MBC_FP64_MATVEC_SIMT;
+  mbc_factor_tiles tiles{{32, 64, 128}, {64, 32, 32, 8}};  // factor class bounds and panel rows
   bool oz_ready = false;  // INT8 digit planes of G built for the current geometry
   mutable bool oz_unprepared = false;  // an INT8 launch found its buffers unsized (not run)
   bool oz_slab = false;   // planes rebuilt per matvec, slab by slab (they do not all fit)

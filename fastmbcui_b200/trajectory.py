@@ -24,6 +24,11 @@ space, so slowly converging columns borrow the directions the others found;
 "mixed" and "fp64" modes) or "batched" (independent per-column recurrences
 advanced together).
 
+Factor tile shapes (``factor_tiles``): a dict for mbc_solver_set_factor_tiles,
+None for the library's defaults, or "tuned" (the default): the table the
+autotuner (fastmbcui_b200.tune_factor) picked on the 32-ellipsoid trajectory
+scene, data/factor_tiles_b200.json, when present.
+
 Warm starts (``warm``): "extrapolate" (quadratic extrapolation of the last
 three steps' strengths, linear with two, the previous with one), "previous",
 "cold" (x0 = 0), or a callable ``warm(history) -> X0 or None``.
@@ -31,9 +36,22 @@ Every column is still decided on its own FP64 residual, whatever the start.
 """
 from __future__ import annotations
 
+import json
+import os
+
 from . import MBC_F32, MBC_F64, MBC_SCHED_BATCHED, MBC_SCHED_BLOCK, Solver
 
 MODES = ("mixed", "fp64", "fp32-replace")
+TUNED_TILES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "factor_tiles_b200.json")
+
+
+def tuned_tiles():
+    """The committed autotuner table, or None."""
+    try:
+        with open(TUNED_TILES) as f:
+            return json.load(f)["tiles"]
+    except (OSError, KeyError, ValueError):
+        return None
 
 
 def extrapolate(hist):
@@ -50,13 +68,14 @@ def extrapolate(hist):
 class TrajectorySolver:
     def __init__(self, coef: float, *, mode: str = "mixed", fp64_matvec: str = "int8",
                  warm="extrapolate", tol: float = 1e-8, max_iters: int = 3000, check_every: int = 8,
-                 compact: bool = False, matvec: int = 0, schedule: str = "block"):
+                 compact: bool = False, matvec: int = 0, schedule: str = "block", factor_tiles="tuned"):
         if mode not in MODES:
             raise ValueError(f"mode must be one of {MODES}")
         self.coef, self.mode, self.fp64_matvec = float(coef), mode, fp64_matvec
         self.warm, self.tol, self.max_iters = warm, float(tol), int(max_iters)
         self.check_every, self.compact, self.matvec = int(check_every), bool(compact), int(matvec)
         self.schedule = {"block": MBC_SCHED_BLOCK, "batched": MBC_SCHED_BATCHED}[schedule]
+        self.factor_tiles = tuned_tiles() if factor_tiles == "tuned" else factor_tiles
         self.history = []
 
     def start(self):
@@ -78,6 +97,8 @@ class TrajectorySolver:
         else:
             s = Solver(plan, x=x, nx=nx, y=y, coef=self.coef, precision=MBC_F32)
             s.set_matvec(self.matvec)
+        if self.factor_tiles:
+            s.set_factor_tiles(self.factor_tiles)
         return s.set_fp64_matvec(self.fp64_matvec).factor()
 
     def step(self, plan, x, nx, y, F, *, X0=None, profile: int = 0, keep: bool = True):

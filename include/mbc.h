@@ -137,6 +137,31 @@ mbc_status mbc_solver_factor(mbc_solver *s, mbc_stream stream);
  * theta[theta_nnz] (per supernode, reversed, column-major, U in the upper part;
  * NULL to skip).  Values are widened to double. */
 mbc_status mbc_solver_get_factor(const mbc_solver *s, double *lval_host, double *theta_host);
+/* Tile shapes of the factor kernels.  Supernodes are split by their row-set
+ * size n_s into four classes: n_s <= max_ns[0] (128 threads), <= max_ns[1]
+ * (256), <= max_ns[2] (512), each with Theta_s in shared memory, and larger
+ * ones (512 threads, Theta_s in global memory).  tile_rows[c] is how many
+ * collocation rows of the K panel a class stages per pass (class 3, and any
+ * class whose shared memory would not fit, use at most that many).  The
+ * shapes change the order of the Gram sums (results agree to rounding), not
+ * the method.  No counterpart in the reference (one thread per supernode,
+ * kl_chol.cu:166-223). */
+typedef struct {
+  int32_t max_ns[3];    /* increasing, 1 .. 144 */
+  int32_t tile_rows[4]; /* 1 .. 256 */
+} mbc_factor_tiles;
+
+void mbc_factor_default_tiles(mbc_factor_tiles *tiles);
+mbc_status mbc_solver_set_factor_tiles(mbc_solver *s, const mbc_factor_tiles *tiles);
+mbc_status mbc_solver_get_factor_tiles(const mbc_solver *s, mbc_factor_tiles *tiles);
+/* Autotuner: factor this solver `reps` times with each candidate tile shape
+ * (class bounds first, then the panel rows of each class in turn, keeping the
+ * best so far), time every factor with CUDA events on `stream`, and leave the
+ * fastest shapes set on the solver.  best (optional) receives them and
+ * ms_best (optional) the best factor time in ms.  The solver ends factored. */
+mbc_status mbc_solver_tune_factor(mbc_solver *s, int32_t reps, mbc_factor_tiles *best,
+                                  double *ms_best, mbc_stream stream);
+
 /* Number of supernodes refactored in FP64 (FP32 solvers: cancelling or
  * non-positive pivots; FP64 solvers: the diagonal-shift retry). */
 mbc_status mbc_solver_get_pivot_retries(const mbc_solver *s, int32_t *count);

@@ -92,7 +92,7 @@ def test_struct_layouts_match_header(tmp_path):
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     mirrors = {"mbc_plan_options": _lib.PlanOptions, "mbc_plan_info": _lib.PlanInfo,
                "mbc_operator": _lib.Operator, "mbc_solve_options": _lib.SolveOptions,
-               "mbc_solve_stats": _lib.SolveStats}
+               "mbc_solve_stats": _lib.SolveStats, "mbc_factor_tiles": _lib.FactorTiles}
     cfield = {"lambda_": "lambda"}  # Python keywords carry a trailing underscore in the mirrors
     lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "mbc.h"', "int main(void) {"]
     for cname, py in mirrors.items():
