@@ -377,7 +377,7 @@ def _plain_leg(args, F, plan, sc, t, R):
         plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
     x, nx, y = t(sc.x), t(sc.nx), t(sc.y)
     Fd = t(sc.rhs(), torch.float64)
-    fx = _oracle_fixture()
+    fx = _oracle_fixture() if args.workload == "trajectory32" else None
     order = list(fx["columns"]) if fx else []
     order += [c for c in np.linspace(0, R - 1, 8).astype(int).tolist() if c not in order]
     plain = F.Solver(plan, x=x, nx=nx, y=y, coef=sc.coef, precision=F.MBC_F64)
@@ -391,7 +391,7 @@ def _plain_leg(args, F, plan, sc, t, R):
     cols, its, ms = [], [], []
     t_leg = time.perf_counter()
     for c in order:
-        if len(cols) >= 2 and (time.perf_counter() - t_leg > args.plain_s or _left(args) < 120):
+        if len(cols) >= args.plain_min and (time.perf_counter() - t_leg > args.plain_s or _left(args) < 120):
             break
         ev0.record()
         _, _, it1 = plain.solve(Fd[:, c].contiguous(), tol=1e-8, max_iters=args.max_iters, check_every=8,
@@ -712,12 +712,14 @@ def run_uneven(args):
     plans = F.plan_many([(sc.y, sc.rho, sc.lam, sc.max_super) for sc in scs])
     data = [(t(sc.x), t(sc.nx), t(sc.y), t(sc.rhs())) for sc in scs]
     fp64 = args.solver == "fp64"
-    opts = dict(out_dtype=torch.float64 if fp64 else torch.float32, tol=1e-8, max_iters=args.max_iters,
+    rec64 = args.solver in ("fp64", "mixed64")  # FP64 recursion (block PCG)
+    opts = dict(out_dtype=torch.float64 if rec64 else torch.float32, tol=1e-8, max_iters=args.max_iters,
                 check_every=8, graph=1)
-    if not fp64:
-        opts.update(max_refine=64, inner_tol=1e-2)
+    if rec64:
+        opts.update(compact=int(args.compact), fp64_recursion=1,
+                    schedule=F.MBC_SCHED_BLOCK if args.schedule == "block" else F.MBC_SCHED_BATCHED)
     else:
-        opts.update(compact=int(args.compact))
+        opts.update(max_refine=64, inner_tol=1e-2)
 
     def step():
         solvers = [F.Solver(pl, x=x, nx=nx, y=y, coef=sc.coef, precision=F.MBC_F64 if fp64 else F.MBC_F32)
@@ -740,7 +742,8 @@ def run_uneven(args):
            "data": "synthetic (seeded scenes)",
            "config": {"workload": "uneven", "scenes": len(scs), "N": [sc.n for sc in scs],
                       "R": [_ncols(sc) for sc in scs], "timing": "host wall clock around the whole sample",
-                      "solver": "FP64 PCG" if fp64 else "mixed FP32/FP64", "fp64_matvec": args.fp64_matvec},
+                      "solver": PRECISION[args.solver], "schedule": SCHEDULE[args.schedule],
+                      "fp64_matvec": args.fp64_matvec},
            "solve": {"iters_max": [int(r[1]["iters_max"]) for r in res],
                      "n_converged": [int(r[1]["n_converged"]) for r in res],
                      "true_relres_max": max(r[1]["true_relres_max"] for r in res)}}
@@ -748,9 +751,17 @@ def run_uneven(args):
 
 
 def run_ours(args):
+    """One pose of a static workload (sphere, coins16, ellipsoids8/32, large):
+    one step = a new factor and the solve of all rigid-mode columns from
+    x0 = 0 with the trajectory solver's configuration (FP32 factor, FP64
+    block PCG, FP64-accurate INT8 matvec; for the large scene the digit
+    planes do not fit and are rebuilt slab by slab for every matvec).  The
+    host plan is its own column; the FP64 true residual of the result is
+    checked with the FP64 CUDA-core kernels."""
     import torch
 
     import fastmbcui_b200 as F
+    from fastmbcui_b200.trajectory import TrajectorySolver
 
     dist, rank, world, local = _dist()
     torch.cuda.set_device(local)
@@ -760,113 +771,102 @@ def run_ours(args):
     Fm = sc.rhs()
     R = Fm.shape[1]
     t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
-
-    # host plan (ordering, pattern, supernodes): reported as its own column
     t0 = time.perf_counter()
     plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
     t_plan = time.perf_counter() - t0
     x, nx, y, Fd = t(sc.x), t(sc.nx), t(sc.y), t(Fm)
-    solver = F.Solver(plan, x=x, nx=nx, y=y, coef=sc.coef, precision=F.MBC_F32)
-    solver.set_matvec(MATVEC[args.matvec]).set_fp64_matvec(args.fp64_matvec)
-    opts = dict(tol=1e-8, max_iters=args.max_iters, max_refine=64, inner_tol=1e-2, check_every=8,
-                compact=int(args.compact))
+    mode = {"mixed64": "mixed", "mixed": "fp32-replace"}.get(args.solver, args.solver)
+    ts = TrajectorySolver(sc.coef, mode=mode, fp64_matvec=args.fp64_matvec, warm="cold",
+                          max_iters=args.max_iters, compact=args.compact, matvec=MATVEC[args.matvec],
+                          schedule=args.schedule)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
-
-    def step(profile=0):
-        solver.factor()
-        return solver.solve(Fd, out_dtype=torch.float32, profile=profile, **opts)
-
     for _ in range(args.warmup):
-        step()
+        ts.step(plan, x, nx, y, Fd, keep=False)
+        if _left(args) < args.budget_s * 0.6:
+            break
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     times, stats = [], []
+    X = None
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             flush.fill_(float(k))
             if dist:
                 dist.barrier()
             torch.cuda.synchronize()
+            t_wall = time.perf_counter()
             ev0.record()
-            X, st = step(profile=1)
+            X, st = ts.step(plan, x, nx, y, Fd, profile=1, keep=False)
             ev1.record()
             torch.cuda.synchronize()
             times.append(ev0.elapsed_time(ev1))
             stats.append(st)
+            stop = _left(args) - 1.5 * (time.perf_counter() - t_wall) < args.reserve_s
+            if dist:
+                flag = torch.tensor([1.0 if stop else 0.0], device=dev)
+                dist.broadcast(flag, 0)
+                stop = bool(flag.item())
+            if stop:
+                break
     ms_step = _max_over_ranks(dist, float(np.mean(times)))
     value = world * 1000.0 / ms_step
+    # FP64 true residual of the result (FP64 CUDA-core kernels)
+    s64 = F.Solver(plan, x=x, nx=nx, y=y, coef=sc.coef, precision=F.MBC_F64)
+    F64 = Fd.double()
+    b = s64.apply_KT(F64)
+    r = s64.apply_KT(F64 - s64.apply_K(X.double()))
+    nb = torch.linalg.norm(b, dim=0)
+    relres = float((torch.linalg.norm(r, dim=0) / torch.clamp(nb, min=1e-300))[nb > 0].max())
+    del s64, r, b
 
     # end to end through the public API: host buffers in, host result out
-    xh, nxh, yh = (np.ascontiguousarray(a, np.float32) for a in (sc.x, sc.nx, sc.y))
-    pin = lambda a: torch.from_numpy(a).pin_memory()
-    hx, hnx, hy, hF = pin(xh), pin(nxh), pin(yh), pin(np.ascontiguousarray(Fm, np.float32))
-    hX = torch.empty((sc.n, R), dtype=torch.float32).pin_memory()
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory()
+    hx, hnx, hy, hF = pin(sc.x), pin(sc.nx), pin(sc.y), pin(Fm)
+    hX = torch.empty((sc.n, R), dtype=torch.float64).pin_memory()
     e2e_ms = []
-    for k in range(max(1, args.e2e_steps)):
+    for k in range(max(1, args.e2e_steps) if _left(args) > args.reserve_s * 0.7 else 0):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         dx, dnx, dy, dF = (a.to(dev, non_blocking=True) for a in (hx, hnx, hy, hF))
-        pl2 = F.Plan(yh.astype(np.float64), sc.rho, sc.lam, sc.max_super)
-        s2 = F.Solver(pl2, x=dx, nx=dnx, y=dy, coef=sc.coef, precision=F.MBC_F32)
-        s2.set_matvec(MATVEC[args.matvec]).factor()
-        X2, _ = s2.solve(dF, out_dtype=torch.float32, **opts)
+        pl2 = F.Plan(sc.y.astype(np.float64), sc.rho, sc.lam, sc.max_super)
+        X2, _ = ts.step(pl2, dx, dnx, dy, dF, keep=False)
         hX.copy_(X2)
         torch.cuda.synchronize()
         e2e_ms.append((time.perf_counter() - t0) * 1000)
-        del s2, pl2
-    e2e = world * 1000.0 / _max_over_ranks(dist, float(np.mean(e2e_ms)))
-    h2d = (xh.nbytes + nxh.nbytes + yh.nbytes + Fm.size * 4)
-    d2h = sc.n * R * 4
-
-    # plain FP64 GPU path: one cold-started PCG per column; bounded sample of
-    # columns, extrapolated to all R (each column is an independent solve)
-    plain = F.Solver(plan, x=x, nx=nx, y=y, coef=sc.coef, precision=F.MBC_F64)
-    ncol = min(R, args.plain_cols)
-    cols = np.linspace(0, R - 1, ncol).astype(int)
-    torch.cuda.synchronize()
-    ev0.record()
-    plain.factor()
-    ev1.record()
-    torch.cuda.synchronize()
-    t_fac64 = ev0.elapsed_time(ev1)
-    ev0.record()
-    Xp, stp = plain.solve(t(Fm[:, cols], torch.float64), tol=1e-8, max_iters=args.max_iters,
-                          schedule=F.MBC_SCHED_PER_RHS, check_every=8)
-    ev1.record()
-    torch.cuda.synchronize()
-    t_cols = ev0.elapsed_time(ev1)
-    plain_ms = t_fac64 + t_cols * R / ncol
-    plain_sps = 1000.0 / _max_over_ranks(dist, plain_ms)
-
+        del X2, pl2
+    e2e = world * 1000.0 / _max_over_ranks(dist, float(np.mean(e2e_ms))) if e2e_ms else None
     st = stats[-1]
-    roofline = _matvec_roofline(st, sc.nf, sc.n, R, args.matvec, args.fp64_matvec)
     out = {
         "metric": METRIC, "value": round(value, 5), "unit": "solves/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": _dtype(args),
-        "data": "synthetic (seeded scene)",
+        "steps": len(times), "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": _dtype(args, args.solver in ("fp64", "mixed64")), "data": "synthetic (seeded scene)",
         "config": {"workload": args.workload, "desc": desc, "N": sc.n, "Nf": sc.nf, "R": R,
-                   "rho": sc.rho, "lambda": sc.lam, "tol": 1e-8, "precision": "mixed FP32/FP64 refine",
-                   "schedule": "batched", "learned_warm_start": False,
+                   "rho": sc.rho, "lambda": sc.lam, "max_super": sc.max_super, "tol": 1e-8,
+                   "precision": PRECISION[args.solver], "schedule": SCHEDULE[args.schedule],
+                   "warm_start": "x0 = 0 (one pose)", "steps_requested": args.steps,
                    "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas{world}"},
-        "e2e": {"value": round(e2e, 5), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "includes": "H2D, host plan, factor, solve, D2H"},
-        "gpu_launches": int(st["kernel_launches"]) + 4 * 10,
-        "plain_fp64": {"solves_per_s": round(plain_sps, 6), "ms_per_solve": round(plain_ms, 1),
-                       "sample": f"{ncol} of {R} columns, per-RHS cold start, extrapolated",
-                       "iters_max": int(stp["iters_max"])},
-        "speedup_vs_plain_fp64": round(value / plain_sps, 2),
-        "solve": {"iters_max": int(st["iters_max"]), "refinements": int(st["refinements"]),
-                  "true_relres_max": st["true_relres_max"], "n_converged": int(st["n_converged"])},
+        "e2e": ({"value": round(e2e, 5), "unit": "solves/s", "h2d_bytes_per_step": int(hx.numel() * 4 * 3 + hF.numel() * 4),
+                 "d2h_bytes_per_step": int(hX.numel() * 8), "includes": "H2D, host plan, factor, solve, D2H"}
+                if e2e else {"skipped": "wall-clock budget"}),
+        "gpu_launches": int(st["kernel_launches"]),
+        "solve": {"iters_max": [int(s_["iters_max"]) for s_ in stats],
+                  "iters_total": [int(s_["iters_total"]) for s_ in stats],
+                  "n_converged": [int(s_["n_converged"]) for s_ in stats],
+                  "fp64_true_relres_max": relres, "ms": [round(v, 1) for v in times]},
         "host_plan_ms": round(t_plan * 1000, 1),
-        "roofline": roofline,
+        "roofline": _matvec_roofline(st, sc.nf, sc.n, R, args.matvec, args.fp64_matvec),
         "clocks": clk.summary(),
     }
-    if rank == 0 and world == 1 and not args.no_cpu:
-        out["cpu_baseline"] = cpu_baseline(sc, st, plan)
+    if _left(args) > args.reserve_s * 0.5 and args.plain_s > 0:
+        out["plain_fp64"] = _plain_leg(args, F, plan, sc, t, R)
+        if out["plain_fp64"].get("solves_per_s"):
+            out["speedup_vs_plain_fp64"] = round(value / out["plain_fp64"]["solves_per_s"], 2)
+    if rank == 0 and world == 1 and not args.no_cpu and _left(args) > 60:
+        out["cpu_baseline"] = cpu_baseline(sc, {"iters_total": st["iters_total"], "source": "this run's GPU solve"})
+    out["wall_s"] = round(time.perf_counter() - T_START, 1)
     if rank == 0:
         print(json.dumps(out), flush=True)
-    del solver, plain
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -1075,6 +1075,7 @@ def main():
     ap.add_argument("--plain-cols", type=int, default=2)
     ap.add_argument("--plain-s", type=float, default=90.0,
                     help="trajectory: seconds for the plain FP64 leg's per-column solves (at least two columns)")
+    ap.add_argument("--plain-min", type=int, default=2, help="plain FP64 leg: at least this many columns")
     ap.add_argument("--ablation", type=int, default=1, help="trajectory: 1 = time the ablation of the speed-up")
     ap.add_argument("--e2e-steps", type=int, default=2)
     # the plain FP64 PCG's iterations per column on the 32-ellipsoid scene
