@@ -1279,14 +1279,24 @@ mbc_status Solver::solve_plain(int R, const void *rhs, int32_t rhs_dt, void *X, 
                                                                              (const T *)fm.ptr, (T *)fsub.ptr);
         launches += 3;
         MBC_CKL();
+        // the last restart runs on the FP64 CUDA-core matvec: a column the
+        // INT8 operator's ~1e-9 product error keeps above tol (near-singular
+        // kernels: sources close to a thin body) converges there, at a cost
+        // proportional to the few columns left
+        const bool last = pass == 1;
+        const double ptol = last ? o.tol : rtol;
+        if (last) fp64_matvec = MBC_FP64_MATVEC_SIMT;
+        mbc_status prs;
         if (precision == MBC_F64)
-          MBC_TRY((run_pcg<T, double, T>(*this, Rs, ws, ws.X, (const double *)lval.ptr, o.max_iters, rtol,
-                                         o.precondition != 0, std::max(1, o.check_every), nullptr, st, d_b2s,
-                                         nullptr, 0, compact)));
+          prs = run_pcg<T, double, T>(*this, Rs, ws, ws.X, (const double *)lval.ptr, o.max_iters, ptol,
+                                      o.precondition != 0, std::max(1, o.check_every), nullptr, st, d_b2s,
+                                      nullptr, 0, compact);
         else
-          MBC_TRY((run_pcg<T, float, T>(*this, Rs, ws, ws.X, (const float *)lval.ptr, o.max_iters, rtol,
-                                        o.precondition != 0, std::max(1, o.check_every), nullptr, st, d_b2s,
-                                        nullptr, 0, compact)));
+          prs = run_pcg<T, float, T>(*this, Rs, ws, ws.X, (const float *)lval.ptr, o.max_iters, ptol,
+                                     o.precondition != 0, std::max(1, o.check_every), nullptr, st, d_b2s,
+                                     nullptr, 0, compact);
+        fp64_matvec = impl;
+        MBC_TRY(prs);
         std::vector<int32_t> it2(Rs);
         MBC_CK(cudaMemcpyAsync(it2.data(), ws.sc.iters, sizeof(int32_t) * Rs, cudaMemcpyDeviceToHost, st));
         // the restarted columns' x back, and their own decision residual
