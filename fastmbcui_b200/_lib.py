@@ -83,6 +83,7 @@ SIGNATURES = {
     "mbc_plan_get_supernodes": (C.c_int, [_vp, _vp, _vp, _vp]),
     "mbc_plan_get_factor_pattern": (C.c_int, [_vp, _vp, _vp]),
     "mbc_spatial_order": (C.c_int, [_i32, _vp, _i32, _vp]),
+    "mbc_minvf_grad": (C.c_int, [_i32, _i32, _i32, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp]),
     "mbc_factor_default_tiles": (None, [C.POINTER(FactorTiles)]),
     "mbc_solver_set_factor_tiles": (C.c_int, [_vp, C.POINTER(FactorTiles)]),
     "mbc_solver_get_factor_tiles": (C.c_int, [_vp, C.POINTER(FactorTiles)]),

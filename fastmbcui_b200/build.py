@@ -26,7 +26,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr
                      "-Xptxas", "-warn-spills"]
 
 HOST_SRC = ["plan.cpp", "capi.cpp", "spatial.cpp"]
-CUDA_SRC = ["solver.cu", "context.cu", "noalloc.cu", "mlp.cu", "warmstart.cu", "mesh.cu", "int8_ops.cu"]
+CUDA_SRC = ["solver.cu", "context.cu", "noalloc.cu", "mlp.cu", "warmstart.cu", "mesh.cu", "int8_ops.cu", "grad.cu"]
 
 
 def _nvcc() -> str:

@@ -146,19 +146,31 @@ def _setup_context(ctx, inputs, output):
 
 
 def _backward(ctx, grad):
-    """grad_M = -M (W + W^T) + F LV, grad_F = M VpL (core/mfs_torch_py/ops.py:42-58)."""
+    """grad_M = -M (W + W^T) + F LV, grad_F = M VpL (core/mfs_torch_py/ops.py:42-58),
+    W = A LV, LV = VpL^T; computed in the equal low-rank form
+    grad_M = (F - M A) VpL^T - (M VpL) A^T by the library's kernels
+    (mbc_minvf_grad), without the N x N matrix W."""
     grad_M, grad_F = None, None
-    if ctx.needs_input_grad[0] or ctx.needs_input_grad[1]:
-        M, F, Vs_s, A = ctx.saved_tensors
-        VpL = torch.ops.mfs_torch.VpL_fast_float.default(M, grad, Vs_s, ctx.rho, ctx.pcg_max_iter,
-                                                         ctx.tol_r, ctx.timing_verbose,
-                                                         ctx.solve_verbose)
+    if not (ctx.needs_input_grad[0] or ctx.needs_input_grad[1]):
+        return grad_M, grad_F, None, None, None, None, None, None
+    M, F, Vs_s, A = ctx.saved_tensors
+    VpL = torch.ops.mfs_torch.VpL_fast_float.default(M, grad, Vs_s, ctx.rho, ctx.pcg_max_iter,
+                                                     ctx.tol_r, ctx.timing_verbose,
+                                                     ctx.solve_verbose)
+    M, F, A, VpL = (t.contiguous() for t in (M, F, A, VpL))
+    nf, n = M.shape
+    R = A.shape[1]
+    work = torch.empty((nf, 2 * R), dtype=torch.float32, device=M.device)
     if ctx.needs_input_grad[0]:
-        LV = VpL.T
-        W = A @ LV
-        grad_M = -M @ (W + W.T) + F @ LV
+        grad_M = torch.empty_like(M)
     if ctx.needs_input_grad[1]:
-        grad_F = M @ VpL
+        grad_F = torch.empty_like(F)
+    st = C.c_void_p(torch.cuda.current_stream(M.device).cuda_stream)
+    _lib.check(_lib.load().mbc_minvf_grad(nf, n, R, M.data_ptr(), M.stride(0), F.data_ptr(), A.data_ptr(),
+                                          VpL.data_ptr(), work.data_ptr(),
+                                          None if grad_M is None else grad_M.data_ptr(), n,
+                                          None if grad_F is None else grad_F.data_ptr(), st),
+               "mbc_minvf_grad")
     return grad_M, grad_F, None, None, None, None, None, None
 
 

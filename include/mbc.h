@@ -394,6 +394,18 @@ mbc_status mbc_minvf_float(mbc_context *ctx, const float *M, int32_t nf, int32_t
                            int64_t pcg_max_iter, double tol_r, int32_t timing_verbose,
                            int32_t solve_verbose, float *out, mbc_stream stream);
 
+/* Gradients of MinvF_float_fastGrad (the reference's autograd,
+ * core/mfs_torch_py/ops.py:42-58: grad_M = -M (W + W^T) + F LV, grad_F = M VpL,
+ * W = A LV, LV = VpL^T) in low-rank form, without the N x N matrix W:
+ *   G = M [A | VpL] (nf x 2R, into work), grad_F = M VpL,
+ *   grad_M = (F - M A) VpL^T - (M VpL) A^T.
+ * M: device nf x n float32 (row stride ldm); F: nf x R; A (the forward's
+ * output) and VpL: n x R; work: device nf x 2R floats; grad_M (row stride ldg)
+ * and grad_F may each be NULL to skip.  FP32 like the reference's products. */
+mbc_status mbc_minvf_grad(int32_t nf, int32_t n, int32_t R, const float *M, int64_t ldm, const float *F,
+                          const float *A, const float *VpL, float *work, float *grad_M, int64_t ldg,
+                          float *grad_F, mbc_stream stream);
+
 mbc_status mbc_vpl_fast_float(mbc_context *ctx, const float *M, int32_t nf, int32_t n,
                               const float *pL, int32_t R, const float *Vs_host, double rho,
                               int64_t pcg_max_iter, double tol_r, int32_t timing_verbose,
