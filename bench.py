@@ -210,13 +210,9 @@ def run_trajectory(args):
     # not the plain method) the ordering, pattern and supernodes of a step are
     # reused for the next K - 1 steps and only the factor is rebuilt, on the
     # current geometry
+    planner = TrajectorySolver(base.coef, plan_every=args.plan_every)
     t0 = time.perf_counter()
-    plans = []
-    for k, sc in enumerate(scenes[:nsteps]):
-        if k % max(1, args.plan_every) == 0:
-            plans.append(F.Plan(sc.y, sc.rho, sc.lam, sc.max_super))
-        else:
-            plans.append(plans[-1])
+    plans = [planner.plan_for(sc.y, sc.rho, sc.lam, sc.max_super) for sc in scenes[:nsteps]]
     t_plan = (time.perf_counter() - t0) / nsteps
     coords = [(t(sc.x), t(sc.nx), t(sc.y)) for sc in scenes[:nsteps]]  # inputs resident in HBM
     Fm = [t(sc.rhs()) for sc in scenes[:nsteps]]

@@ -29,6 +29,14 @@ None for the library's defaults, or "tuned" (the default): the table the
 autotuner (fastmbcui_b200.tune_factor) picked on the 32-ellipsoid trajectory
 scene, data/factor_tiles_b200.json, when present.
 
+Ordering reuse (``plan_every``): the host plan (maximin ordering, pattern,
+supernodes) of a step is rebuilt every ``plan_every`` steps (1, the default,
+is the plain method: a new plan per call, as mfs_torch_ops.cu:51-55 and
+:114-116 build one); with K > 1 the plan of a step is reused for the next
+K - 1 steps of slowly moving bodies while the factor is always rebuilt on the
+current geometry.  That changes the preconditioner, not the solution, which
+every column's own FP64 residual still decides.
+
 Warm starts (``warm``): "extrapolate" (quadratic extrapolation of the last
 three steps' strengths, linear with two, the previous with one), "previous",
 "cold" (x0 = 0), or a callable ``warm(history) -> X0 or None``.
@@ -68,7 +76,8 @@ def extrapolate(hist):
 class TrajectorySolver:
     def __init__(self, coef: float, *, mode: str = "mixed", fp64_matvec: str = "int8",
                  warm="extrapolate", tol: float = 1e-8, max_iters: int = 3000, check_every: int = 8,
-                 compact: bool = False, matvec: int = 0, schedule: str = "block", factor_tiles="tuned"):
+                 compact: bool = False, matvec: int = 0, schedule: str = "block", factor_tiles="tuned",
+                 plan_every: int = 1):
         if mode not in MODES:
             raise ValueError(f"mode must be one of {MODES}")
         self.coef, self.mode, self.fp64_matvec = float(coef), mode, fp64_matvec
@@ -76,7 +85,21 @@ class TrajectorySolver:
         self.check_every, self.compact, self.matvec = int(check_every), bool(compact), int(matvec)
         self.schedule = {"block": MBC_SCHED_BLOCK, "batched": MBC_SCHED_BATCHED}[schedule]
         self.factor_tiles = tuned_tiles() if factor_tiles == "tuned" else factor_tiles
+        if int(plan_every) < 1:
+            raise ValueError("plan_every must be >= 1")
+        self.plan_every = int(plan_every)
+        self._plan, self._plan_age = None, 0
         self.history = []
+
+    def plan_for(self, pts, rho: float, lam: float, max_super: int):
+        """The host plan for this step's source points (n x 3): a new one
+        every plan_every steps, else the last one."""
+        from . import Plan
+
+        if self._plan is None or self._plan_age >= self.plan_every:
+            self._plan, self._plan_age = Plan(pts, rho, lam, max_super), 0
+        self._plan_age += 1
+        return self._plan
 
     def start(self):
         """The warm start of the next step (None: x0 = 0)."""
