@@ -108,12 +108,24 @@ class Solver:
     """
 
     def __init__(self, plan: Plan, *, M=None, x=None, nx=None, y=None, coef: float = 1.0,
-                 precision: int = MBC_F64, stream=None):
+                 precision: int = MBC_F64, stream=None, mesh=None):
+        """Operator: a dense M (nf x n float32), the point kernel (x, nx: nf x 3;
+        y: n x 3), or mesh=(V, faces, S): the matrix-free mesh collocation
+        operator (solid angle of each face seen from each source; V: n_vert x
+        3 float, faces: nf x 3 int32, S: n x 3), all CUDA tensors."""
         import torch
 
         L = load()
         op = _lib.Operator()
-        if M is not None:
+        if mesh is not None:
+            V, Fc, Sy = mesh
+            V, Sy = V.contiguous().float(), Sy.contiguous().float()
+            Fc = Fc.contiguous().to(torch.int32)
+            op.kind, op.nf, op.n = _lib.MBC_OP_MESH, Fc.shape[0], Sy.shape[0]
+            op.V, op.faces, op.n_vert, op.y = V.data_ptr(), Fc.data_ptr(), V.shape[0], Sy.data_ptr()
+            op.coef = float(coef)
+            self._keep = (V, Fc, Sy)
+        elif M is not None:
             assert M.is_cuda and M.dtype == torch.float32 and M.dim() == 2
             M = M.contiguous()
             op.kind, op.nf, op.n, op.M, op.ldm = MBC_OP_DENSE, M.shape[0], M.shape[1], M.data_ptr(), M.shape[1]

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(PKG, "libmbc.so")
 MBC_OK, MBC_NOT_CONVERGED, MBC_BREAKDOWN, MBC_NONSPD_PIVOT, MBC_BAD_ARG = 0, 1, 2, 3, 4
 MBC_CUDA_ERROR, MBC_TIMEOUT, MBC_NO_MEMORY, MBC_COVERAGE, MBC_UNSUPPORTED = 5, 6, 7, 8, 9
 MBC_F64, MBC_F32 = 0, 1
-MBC_OP_DENSE, MBC_OP_POINT_KERNEL = 0, 1
+MBC_OP_DENSE, MBC_OP_POINT_KERNEL, MBC_OP_MESH = 0, 1, 2
 MBC_SCHED_BATCHED, MBC_SCHED_PER_RHS, MBC_SCHED_BLOCK = 0, 1, 2
 MBC_MATVEC_AUTO, MBC_MATVEC_SIMT, MBC_MATVEC_TENSOR = 0, 1, 2
 MBC_FP64_MATVEC_SIMT, MBC_FP64_MATVEC_INT8 = 0, 1
@@ -38,7 +38,7 @@ class PlanInfo(C.Structure):
 class Operator(C.Structure):
     _fields_ = [("kind", C.c_int32), ("nf", C.c_int32), ("n", C.c_int32), ("M", C.c_void_p),
                 ("ldm", C.c_int64), ("x", C.c_void_p), ("nx", C.c_void_p), ("y", C.c_void_p),
-                ("coef", C.c_double)]
+                ("coef", C.c_double), ("V", C.c_void_p), ("faces", C.c_void_p), ("n_vert", C.c_int32)]
 
 
 class SolveOptions(C.Structure):

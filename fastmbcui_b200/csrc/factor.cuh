@@ -15,6 +15,7 @@
 #include <stdint.h>
 
 #include "matvec.cuh"
+#include "matvec_mesh.cuh"
 
 namespace mbc {
 
@@ -24,8 +25,9 @@ struct FactorArgs {
   const int32_t *sup_ptr, *sup_ind, *set_ptr, *set_ind, *lptr;
   const int64_t *th_ptr;
   // operator
-  int32_t kind;  // 0 dense, 1 point kernel
-  const float4 *xr, *nr, *ys;  // point kernel (ys in the new order)
+  int32_t kind;  // 0 dense, 1 point kernel, 2 mesh (solid angles)
+  const float4 *xr, *nr, *ys;  // point kernel (ys in the new order); mesh: face vertices 1, 2
+  const float4 *zr;            // mesh: face vertex 3
   const float *M;
   int64_t ldm;
   const int32_t *Pinv;  // dense: column of M for each new index
@@ -86,7 +88,7 @@ __global__ void __launch_bounds__(NT) factor_kernel(FactorArgs a, T *__restrict_
 
   for (int p = tid; p < ns; p += NT) {
     const int c = a.set_ind[sb + p];
-    if (a.kind == 1) s_src[p] = a.ys[c];
+    if (a.kind != 0) s_src[p] = a.ys[c];
     else s_col[p] = a.Pinv[c];
   }
   const int ne = ns * (ns + 1) / 2;
@@ -116,6 +118,7 @@ __global__ void __launch_bounds__(NT) factor_kernel(FactorArgs a, T *__restrict_
         const int i = i0 + rr;
         T kv;
         if (a.kind == 1) kv = coef * PointKernel<T>::eval(a.xr[i], a.nr[i], s_src[p]);
+        else if (a.kind == 2) kv = coef * SolidAngle<T>::eval(a.xr[i], a.nr[i], a.zr[i], s_src[p]);
         else kv = (T)__ldg(a.M + (size_t)i * a.ldm + s_col[p]);
         panel[t] = kv;
       }

@@ -17,6 +17,7 @@
 #include "factor.cuh"
 #include "forces.cuh"
 #include "matvec.cuh"
+#include "matvec_mesh.cuh"
 #include "matvec_tc.cuh"
 #include "cuda_util.h"
 #include "int8_ops.h"
@@ -102,6 +103,10 @@ void rows_launch(const Solver &S, int R, const T *v, T *w, const int32_t *done, 
     dim3 grid(cdiv(S.nf, TI), cdiv(R, RC));
     pk_rows_kernel<T, RC, TI, TJ_ROWS><<<grid, TI, 0, st>>>(S.x4(), S.n4(), S.nf, S.y4(), S.n, v, R,
                                                             (T)S.op.coef, w, R, R, done);
+  } else if (S.op.kind == MBC_OP_MESH) {
+    dim3 grid(cdiv(S.nf, TI), cdiv(R, RC));
+    mesh_rows_kernel<T, RC, TI, TJ_ROWS><<<grid, TI, 0, st>>>(S.x4(), S.n4(), S.z4(), S.nf, S.y4(), S.n, v, R,
+                                                              (T)S.op.coef, w, R, R, done);
   } else {
     dim3 grid(cdiv(S.nf, 8), cdiv(R, RC));
     dense_rows_kernel<T, RC><<<grid, 256, 0, st>>>(S.op.M, S.op.ldm, S.nf, S.n, S.dP(), v, R, w,
@@ -117,6 +122,9 @@ int cols_launch(const Solver &S, int R, const T *w, T *t, const T *pdot, double 
   if (S.op.kind == MBC_OP_POINT_KERNEL) {
     pk_cols_kernel<T, RC, TI, TJ_COLS><<<grid, TI, 0, st>>>(S.x4(), S.n4(), S.nf, S.y4(), S.n, w, R,
                                                             (T)S.op.coef, t, R, R, pdot, part, done);
+  } else if (S.op.kind == MBC_OP_MESH) {
+    mesh_cols_kernel<T, RC, TI, TJ_COLS><<<grid, TI, 0, st>>>(S.x4(), S.n4(), S.z4(), S.nf, S.y4(), S.n, w, R,
+                                                              (T)S.op.coef, t, R, R, pdot, part, done);
   } else {
     dense_cols_kernel<T, RC, TI, 32><<<grid, TI, 0, st>>>(S.op.M, S.op.ldm, S.nf, S.n, S.dP(), w, R,
                                                           t, R, R, pdot, part, done);
@@ -194,7 +202,7 @@ void launch_rows(const Solver &S, int R, const T *v, T *w, const int32_t *done, 
     }
   }
   ++S.launches;
-  const Shape sh = pick_shape<T>(S.op.kind == MBC_OP_POINT_KERNEL ? S.nf : 1 << 30, R);
+  const Shape sh = pick_shape<T>(S.op.kind != MBC_OP_DENSE ? S.nf : 1 << 30, R);
 #define MBC_ROWS_CASE(TT, RC_, TI_) \
   if (sh.rc == RC_ && sh.ti == TI_) return rows_launch<T, RC_, TI_>(S, R, v, w, done, st);
   MBC_SHAPES(T, MBC_ROWS_CASE)
@@ -307,6 +315,7 @@ static mbc_status run_factor(Solver &S, const std::vector<int32_t> *lists, T *th
     a.kind = S.op.kind;
     a.xr = S.x4();
     a.nr = S.n4();
+    a.zr = S.z4();
     a.ys = S.y4();
     a.M = S.op.M;
     a.ldm = S.op.ldm;
@@ -448,6 +457,17 @@ mbc_status Solver::create(const Plan &pl, const mbc_operator &o, int32_t prec, c
   MBC_TRY(upload(m_th_ptr, pl.th_ptr, st));
   MBC_TRY(m_err.reserve(sizeof(int32_t)));
   MBC_CK(cudaMemsetAsync(m_err.ptr, 0, sizeof(int32_t), st));
+  if (o.kind == MBC_OP_MESH) {
+    // faces as three vertex arrays (original face order), sources in plan order
+    MBC_TRY(m_x4.reserve(sizeof(float4) * nf));
+    MBC_TRY(m_n4.reserve(sizeof(float4) * nf));
+    MBC_TRY(m_z4.reserve(sizeof(float4) * nf));
+    MBC_TRY(m_y4.reserve(sizeof(float4) * n));
+    pack_faces_kernel<<<cdiv(nf, 256), 256, 0, st>>>(nf, o.V, o.n_vert, o.faces, (float4 *)m_x4.ptr,
+                                                     (float4 *)m_n4.ptr, (float4 *)m_z4.ptr);
+    pack_points_kernel<<<cdiv(n, 256), 256, 0, st>>>(n, o.y, (const int32_t *)m_Pinv.ptr, (float4 *)m_y4.ptr);
+    MBC_CKL();
+  }
   if (o.kind == MBC_OP_POINT_KERNEL) {
     // padded to whole 32-point tiles (the tensor-core path copies whole tiles)
     const size_t nf_pad = (size_t)cdiv(nf, 32) * 32, n_pad = (size_t)cdiv(n, 32) * 32;
@@ -1630,6 +1650,9 @@ extern "C" mbc_status mbc_solver_create(const mbc_plan *plan, const mbc_operator
     if (!op->M || op->ldm < op->n) return fail(MBC_BAD_ARG, "dense operator needs M with ldm >= n");
   } else if (op->kind == MBC_OP_POINT_KERNEL) {
     if (!op->x || !op->nx || !op->y) return fail(MBC_BAD_ARG, "point kernel needs x, nx and y");
+  } else if (op->kind == MBC_OP_MESH) {
+    if (!op->V || !op->faces || !op->y || op->n_vert <= 0)
+      return fail(MBC_BAD_ARG, "mesh operator needs V (n_vert > 0), faces and y");
   } else {
     return fail(MBC_BAD_ARG, "unknown operator kind");
   }

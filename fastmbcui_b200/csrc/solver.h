@@ -51,6 +51,7 @@ struct Solver {
   DevMem class_list[4];
   // operator: rows (original order) and sources (new order) as float4
   DevMem m_x4, m_n4, m_y4;
+  DevMem m_z4;  // mesh operator: third vertex of every face (x4, n4 hold the first two)
   DevMem m_err;           // set by a tensor-core kernel (1: a bounded wait expired)
   mutable DevMem m_bimg;  // packed TF32 hi/lo image of the tensor-core B operand
   // FP64-accurate INT8 matvec: digit planes and exponents of G per direction
@@ -87,6 +88,7 @@ struct Solver {
   const float4 *x4() const { return (const float4 *)m_x4.ptr; }
   const float4 *n4() const { return (const float4 *)m_n4.ptr; }
   const float4 *y4() const { return (const float4 *)m_y4.ptr; }
+  const float4 *z4() const { return (const float4 *)m_z4.ptr; }
 
   mbc_status create(const Plan &pl, const mbc_operator &o, int32_t prec, cudaStream_t st);
   mbc_status ensure_events(int count);

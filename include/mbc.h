@@ -103,7 +103,7 @@ mbc_status mbc_spatial_order(int32_t n, const float *pts_host, int32_t stride, i
 /* ------------------------------------------------------------------------ */
 /* Operator K (nf collocation rows x n source columns).                       */
 /* ------------------------------------------------------------------------ */
-typedef enum { MBC_OP_DENSE = 0, MBC_OP_POINT_KERNEL = 1 } mbc_op_kind;
+typedef enum { MBC_OP_DENSE = 0, MBC_OP_POINT_KERNEL = 1, MBC_OP_MESH = 2 } mbc_op_kind;
 
 typedef struct {
   int32_t kind;
@@ -115,6 +115,15 @@ typedef struct {
    * (src/kernels.h:24-40 with coef = 1).  x, nx: nf x 3; y: n x 3. */
   const float *x, *nx, *y;
   double coef;
+  /* MBC_OP_MESH (matrix-free form of the mesh collocation operator,
+   * utils/torch_utils.py:306-334): K(f, j) = coef * the solid angle of face f
+   * (vertices V[faces[f][0..2]]) seen from source y_j, evaluated on the fly
+   * (the dense matrix mbc_mesh_assemble writes, never stored).  nf = faces;
+   * faces: device nf x 3 int32; V: device n_vert x 3; y: device n x 3.
+   * FP64 and FP32 CUDA-core matvecs (no tensor-core or INT8 form). */
+  const float *V;
+  const int32_t *faces;
+  int32_t n_vert;
 } mbc_operator;
 
 /* ------------------------------------------------------------------------ */

@@ -83,3 +83,59 @@ def test_mesh_operator_feeds_the_drop_in_op():
         xo, _, _ = O.pcg(op, pl, lval, f=R[:, c], maxits=4000, tol=1e-6)
         d = np.linalg.norm(K @ X[:, c] - K @ xo[pl["P"]]) / np.linalg.norm(R[:, c])
         assert d < 1e-3, (c, d)
+
+
+def _mesh_case():
+    m = S.mesh_scene([(3, (1.0, 0.8, 0.6), (0.1, 0.2, 0.3), (0.0, 0.0, 0.0), 0.1),
+                      (3, (0.7, 0.9, 0.5), (0.3, -0.2, 0.1), (2.6, 0.4, -0.2), 0.1)])
+    Mo, rhs = O.mesh_operator(m["V"], m["F"], m["face_body"], m["body_pos"], m["S"])
+    return m, Mo, rhs
+
+
+def test_matrix_free_mesh_operator_products():
+    """The matrix-free mesh operator (MBC_OP_MESH: solid angles evaluated in
+    the matvec) against the oracle's dense FP64 matrix: K and K^T within 1e-12
+    (FP64 solver) and 2e-5 (FP32 solver), norm-wise relative."""
+    import fastmbcui_b200 as F
+
+    m, Mo, _ = _mesh_case()
+    d = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device="cuda")
+    plan = F.Plan(m["S"], 3.0, 1.5, 2048)
+    rng = np.random.default_rng(0)
+    V, W = rng.standard_normal((Mo.shape[1], 5)), rng.standard_normal((Mo.shape[0], 5))
+    for prec, tol, dt in ((F.MBC_F64, 1e-12, torch.float64), (F.MBC_F32, 2e-5, torch.float32)):
+        s = F.Solver(plan, mesh=(d(m["V"]), d(m["F"], torch.int32), d(m["S"])), precision=prec)
+        got_k = s.apply_K(d(V, dt)).double().cpu().numpy()
+        got_kt = s.apply_KT(d(W, dt)).double().cpu().numpy()
+        assert np.linalg.norm(got_k - Mo @ V) / np.linalg.norm(Mo @ V) < tol
+        assert np.linalg.norm(got_kt - Mo.T @ W) / np.linalg.norm(Mo.T @ W) < tol
+
+
+def test_matrix_free_mesh_operator_solve_matches_oracle():
+    """Factor and PCG with the matrix-free mesh operator against the oracle
+    on the same FP64 dense matrix: the KL factor within 1e-7 per column
+    (norm-wise), PCG iterations within max(3, 3 %) per column, and the FP64
+    true residual (dense oracle matrix) <= tol."""
+    import fastmbcui_b200 as F
+
+    m, Mo, rhs = _mesh_case()
+    d = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device="cuda")
+    plan = F.Plan(m["S"], 3.0, 1.5, 2048)
+    pl = O.plan(m["S"], 3.0, 1.5, 2048)
+    op = O.Op(Mo.shape[0], Mo.shape[1], M=Mo)
+    _, lval_o, _ = O.factor(op, pl)
+    s = F.Solver(plan, mesh=(d(m["V"]), d(m["F"], torch.int32), d(m["S"])), precision=F.MBC_F64).factor()
+    lval, _ = s.get_factor()
+    lp = pl["lptr"]
+    for c in range(0, Mo.shape[1], max(1, Mo.shape[1] // 50)):
+        a, b = lp[c], lp[c + 1]
+        assert np.linalg.norm(lval[a:b] - lval_o[a:b]) <= 1e-7 * np.linalg.norm(lval_o[a:b])
+    cols = [c for c in range(rhs.shape[1]) if np.linalg.norm(rhs[:, c]) > 0]
+    X, st, its = s.solve(d(rhs[:, cols], torch.float64), tol=1e-8, max_iters=4000, iters=True)
+    X = X.cpu().numpy()
+    for k, c in enumerate(cols):
+        xo, it, _ = O.pcg(op, pl, lval_o, f=rhs[:, c], maxits=4000, tol=1e-8)
+        assert abs(int(its[k]) - it) <= max(3, 0.03 * it), (c, int(its[k]), it)
+        b = Mo.T @ rhs[:, c]
+        r = Mo.T @ (rhs[:, c] - Mo @ X[:, k])
+        assert np.linalg.norm(r) <= 1.05e-8 * np.linalg.norm(b)
