@@ -144,173 +144,179 @@ __global__ void __launch_bounds__(kThreads) block_update_kernel(int n, int k, in
 }
 
 // ---------------------------------------------------------------------------
-// Small dense kernels: one block of kSmallThreads threads.  With use_smem (the
-// caller passes k * k doubles of dynamic shared memory, k <= kSmemDim) the
-// k x k matrix is staged in shared memory, otherwise it stays in global
-// memory (L1 / L2); the arithmetic and its order are the same either way.
-constexpr int kSmemDim = 152;  // 152^2 doubles = 180.5 KB
+// Small dense kernels.  The k x k matrices are symmetric (Gram matrices) or
+// lower triangular (their Cholesky factors), so only the lower triangle is
+// read or written.  With `packed` the lower triangle is staged in shared
+// memory in packed row order (row i at i (i + 1) / 2), which holds k up to
+// kPackedDim; above that the kernels work on the global copy (L1 / L2).  The
+// arithmetic and its order are the same either way.
+constexpr int kPackedDim = 208;  // 208 * 209 / 2 doubles = 169.8 KB
+constexpr int kSolveWarps = 8;   // columns (one warp each) per block of the column-parallel solves
 
-__device__ __forceinline__ void stage_in(int k, const double *src, int ld, double *dst)
-{
-  for (int64_t t = threadIdx.x; t < (int64_t)k * k; t += blockDim.x) {
-    const int i = (int)(t / k), j = (int)(t % k);
-    dst[t] = src[(size_t)i * ld + j];
+__host__ __device__ constexpr size_t packed_len(int k) { return (size_t)k * (k + 1) / 2; }
+
+// lower-triangle element (i, l), i >= l, of a packed or a row-major matrix
+struct Lower {
+  double *p;
+  int ld;
+  int packed;
+  __device__ __forceinline__ double &operator()(int i, int l) const
+  {
+    return packed ? p[(size_t)i * (i + 1) / 2 + l] : p[(size_t)i * ld + l];
   }
+};
+
+// lower triangle of src (k x k, ld) -> packed dst; every thread of the block
+// takes part and the block is synchronised afterwards
+__device__ __forceinline__ void stage_lower(int k, const double *src, int ld, double *dst)
+{
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int i = threadIdx.x >> 5; i < k; i += nw)
+    for (int l = lane; l <= i; l += 32) dst[(size_t)i * (i + 1) / 2 + l] = src[(size_t)i * ld + l];
   __syncthreads();
 }
 
-// In place lower Cholesky of the k x k SPD matrix G (row-major, ld):
-// G = L L^T, L in the lower triangle (the strict upper triangle is left as
-// is).  *flag = 1 on a pivot that is not positive (or NaN).
-__global__ void __launch_bounds__(kSmallThreads) chol_kernel(int k, double *Gg, int ldg, int32_t *flag,
-                                                             int use_smem)
+// In place lower Cholesky of the k x k SPD matrix G (row-major, ld; lower
+// triangle read): G = L L^T, L written to the lower triangle (the strict
+// upper triangle is left as is).  *flag = 1 on a pivot that is not positive
+// (or NaN).  One block of kSmallThreads; with packed, k (k + 1) / 2 doubles
+// of dynamic shared memory.
+__global__ void __launch_bounds__(kSmallThreads) chol_kernel(int k, double *Gg, int ldg, int32_t *flag, int packed)
 {
   extern __shared__ double sm[];
   __shared__ int bad;
   if (threadIdx.x == 0) bad = 0;
-  double *G = Gg;
-  int ld = ldg;
-  if (use_smem) {
-    stage_in(k, Gg, ldg, sm);
-    G = sm;
-    ld = k;
-  }
+  if (packed) stage_lower(k, Gg, ldg, sm);
+  const Lower G{packed ? sm : Gg, ldg, packed};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   __syncthreads();
   for (int j = 0; j < k; ++j) {
     if (threadIdx.x == 0) {
-      const double d = G[(size_t)j * ld + j];
+      const double d = G(j, j);
       if (!(d > 0.0)) bad = 1;
-      G[(size_t)j * ld + j] = d > 0.0 ? sqrt(d) : 1.0;
+      G(j, j) = d > 0.0 ? sqrt(d) : 1.0;
     }
     __syncthreads();
     if (bad) break;
-    const double djj = G[(size_t)j * ld + j];
-    for (int i = j + 1 + threadIdx.x; i < k; i += blockDim.x) G[(size_t)i * ld + j] /= djj;
+    const double djj = G(j, j);
+    for (int i = j + 1 + threadIdx.x; i < k; i += blockDim.x) G(i, j) /= djj;
     __syncthreads();
-    const int w = k - j - 1;
-    for (int64_t t = threadIdx.x; t < (int64_t)w * w; t += blockDim.x) {
-      const int i = j + 1 + (int)(t / w), l = j + 1 + (int)(t % w);
-      if (l <= i) G[(size_t)i * ld + l] -= G[(size_t)i * ld + j] * G[(size_t)l * ld + j];
+    // trailing update of the lower triangle, one warp per row
+    for (int i = j + 1 + warp; i < k; i += nw) {
+      const double gij = G(i, j);
+      for (int l = j + 1 + lane; l <= i; l += 32) G(i, l) -= gij * G(l, j);
     }
     __syncthreads();
   }
-  if (use_smem)
-    for (int64_t t = threadIdx.x; t < (int64_t)k * k; t += blockDim.x) {
-      const int i = (int)(t / k), j = (int)(t % k);
-      if (j <= i) Gg[(size_t)i * ldg + j] = sm[t];
-    }
+  if (packed) {
+    for (int i = warp; i < k; i += nw)
+      for (int l = lane; l <= i; l += 32) Gg[(size_t)i * ldg + l] = G(i, l);
+  }
   if (threadIdx.x == 0 && bad && flag) *flag = 1;
 }
 
-// B (k x m, ldb) <- sgn * (L L^T)^{-1} B, L lower from chol_kernel; nothing
-// is done when *skip is set (the factorization failed)
-__global__ void __launch_bounds__(kSmallThreads) chol_solve_kernel(int k, const double *Lg, int ldg, int m,
-                                                                   double *B, int ldb, double sgn,
-                                                                   const int32_t *skip, int use_smem)
+// B (k x m, ldb) <- sgn * (L L^T)^{-1} B for the lower factor L of
+// chol_kernel (lower triangle of Lg, ldg).  One warp per column of B,
+// kSolveWarps columns per block, grid cdiv(m, kSolveWarps): forward then
+// backward substitution in the column-oriented order, the column held in
+// shared memory.  Dynamic shared memory: kSolveWarps * k doubles, plus
+// packed_len(k) with packed (L staged).  Nothing is done when *skip is set
+// (the factorization failed).
+__global__ void __launch_bounds__(kSolveWarps * 32) chol_solve_kernel(int k, const double *Lg, int ldg, int m,
+                                                                      double *B, int ldb, double sgn,
+                                                                      const int32_t *skip, int packed)
 {
   extern __shared__ double sm[];
   if (skip && *skip) return;
-  const double *L = Lg;
-  int ld = ldg;
-  if (use_smem) {
-    stage_in(k, Lg, ldg, sm);
-    L = sm;
-    ld = k;
-  }
-  // forward: L y = b
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double *Lp = sm + (size_t)kSolveWarps * k;
+  if (packed) stage_lower(k, Lg, ldg, Lp);
+  const Lower L{packed ? Lp : const_cast<double *>(Lg), ldg, packed};
+  const int c = blockIdx.x * kSolveWarps + warp;
+  if (c >= m) return;
+  double *x = sm + (size_t)warp * k;
+  for (int i = lane; i < k; i += 32) x[i] = B[(size_t)i * ldb + c];
+  __syncwarp();
+  // forward: L y = b.  Every lane reads x[j] before the __syncwarp; lane 0
+  // stores y_j after it (x[j] is read again only in the backward pass).
   for (int j = 0; j < k; ++j) {
-    const double ljj = L[(size_t)j * ld + j];
-    for (int c = threadIdx.x; c < m; c += blockDim.x) B[(size_t)j * ldb + c] /= ljj;
-    __syncthreads();
-    const int w = k - j - 1;
-    for (int64_t t = threadIdx.x; t < (int64_t)w * m; t += blockDim.x) {
-      const int i = j + 1 + (int)(t / m), c = (int)(t % m);
-      B[(size_t)i * ldb + c] -= L[(size_t)i * ld + j] * B[(size_t)j * ldb + c];
-    }
-    __syncthreads();
+    const double yj = x[j] / L(j, j);
+    for (int i = j + 1 + lane; i < k; i += 32) x[i] -= L(i, j) * yj;
+    __syncwarp();
+    if (lane == 0) x[j] = yj;
   }
+  __syncwarp();
   // backward: L^T x = y
   for (int j = k - 1; j >= 0; --j) {
-    const double ljj = L[(size_t)j * ld + j];
-    for (int c = threadIdx.x; c < m; c += blockDim.x) B[(size_t)j * ldb + c] /= ljj;
-    __syncthreads();
-    for (int64_t t = threadIdx.x; t < (int64_t)j * m; t += blockDim.x) {
-      const int i = (int)(t / m), c = (int)(t % m);
-      B[(size_t)i * ldb + c] -= L[(size_t)j * ld + i] * B[(size_t)j * ldb + c];
-    }
-    __syncthreads();
+    const double xj = x[j] / L(j, j);
+    for (int i = lane; i < j; i += 32) x[i] -= L(j, i) * xj;
+    __syncwarp();
+    if (lane == 0) x[j] = xj;
   }
-  if (sgn != 1.0)
-    for (int64_t t = threadIdx.x; t < (int64_t)k * m; t += blockDim.x) {
-      const int i = (int)(t / m), c = (int)(t % m);
-      B[(size_t)i * ldb + c] *= sgn;
-    }
+  __syncwarp();
+  for (int i = lane; i < k; i += 32) B[(size_t)i * ldb + c] = sgn * x[i];
 }
 
 constexpr int kOrthMax = 512;  // widest block orth_factor_kernel takes
 
-// Rank-revealing Cholesky of the m x m Gram matrix W (row-major, ld; destroyed)
-// of a block V (m <= kOrthMax).  The columns are first scaled to unit norm
-// (the span does not change, and a column with a small norm is not mistaken
-// for a dependent one); then, with diagonal pivoting, the factorization
-// stops at the first pivot below drop^2 times the largest scaled diagonal
-// (or, with drop = 0, not above zero).  Writes T (m x m, ldt, its first r
-// columns used) such that V T[:, :r] has orthonormal columns in exact
-// arithmetic: T = D Pi U^{-1}, D the column scaling, Pi^T D W D Pi = U^T U on
-// the kept pivots; and *rank = r.  Work: perm[m] int32.
+// Rank-revealing Cholesky of the m x m Gram matrix W (row-major, ld; lower
+// triangle read, overwritten by the factor) of a block V (m <= kOrthMax).
+// The columns are first scaled to unit norm (the span does not change, and
+// a column with a small norm is not mistaken for a dependent one); then,
+// with diagonal pivoting, the factorization stops at the first pivot below
+// drop^2 times the largest scaled diagonal (or, with drop = 0, not above
+// zero).  Writes the factor L of the kept pivots (Pi^T D W D Pi = L L^T on
+// them) to W's lower triangle in pivoted order, the pivots perm[m], the
+// column scaling scale[m] (D) and *rank = r; orth_t_kernel then forms
+// T = D Pi L^{-T}, with V T[:, :r] orthonormal in exact arithmetic.  One
+// block of kSmallThreads; with packed, packed_len(m) doubles of dynamic
+// shared memory.
 __global__ void __launch_bounds__(kSmallThreads) orth_factor_kernel(int m, double *Wg, int ldg, double drop,
-                                                                    double *T, int ldt, int32_t *perm,
-                                                                    int32_t *rank, int use_smem)
+                                                                    double *scale, int32_t *perm, int32_t *rank,
+                                                                    int packed)
 {
   extern __shared__ double sm[];
-  double *W = Wg;
-  int ld = ldg;
-  if (use_smem) {
-    stage_in(m, Wg, ldg, sm);
-    W = sm;
-    ld = m;
-  }
   __shared__ double s_val[32];
   __shared__ int s_idx[32];
   __shared__ int s_r;
   __shared__ double s_dmax;
   __shared__ double s_scale[kOrthMax];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const Lower W{packed ? sm : Wg, ldg, packed};
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
     perm[i] = i;
-    const double d = W[(size_t)i * ld + i];
+    const double d = Wg[(size_t)i * ldg + i];
     s_scale[i] = d > 0.0 ? 1.0 / sqrt(d) : 0.0;
   }
   __syncthreads();
-  for (int64_t t = threadIdx.x; t < (int64_t)m * m; t += blockDim.x) {
-    const int i = (int)(t / m), l = (int)(t % m);
-    W[(size_t)i * ld + l] *= s_scale[i] * s_scale[l];
-  }
+  // scaled lower triangle (staged when packed)
+  for (int i = warp; i < m; i += nw)
+    for (int l = lane; l <= i; l += 32) W(i, l) = Wg[(size_t)i * ldg + l] * (s_scale[i] * s_scale[l]);
   __syncthreads();
   // largest initial diagonal
   {
     double mx = 0.0;
-    for (int i = threadIdx.x; i < m; i += blockDim.x) mx = fmax(mx, W[(size_t)i * ld + i]);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) mx = fmax(mx, W(i, i));
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     if (lane == 0) s_val[warp] = mx;
     __syncthreads();
     if (threadIdx.x == 0) {
       double v = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v = fmax(v, s_val[w]);
+      for (int w = 0; w < nw; ++w) v = fmax(v, s_val[w]);
       s_dmax = v;
       s_r = m;
     }
     __syncthreads();
   }
   const double thr = drop > 0.0 ? drop * drop * s_dmax : 0.0;
-  // pivoted Cholesky on the symmetric matrix, lower triangle in the permuted
-  // positions: W holds the working matrix with rows / columns swapped in place
+  // pivoted Cholesky of the symmetric matrix on its lower triangle, rows and
+  // columns swapped in place
   for (int j = 0; j < m; ++j) {
     // pivot: the largest remaining diagonal (lowest index on ties)
     double best = -1.0;
     int bi = j;
     for (int i = j + threadIdx.x; i < m; i += blockDim.x) {
-      const double d = W[(size_t)i * ld + i];
+      const double d = W(i, i);
       if (d > best) {
         best = d;
         bi = i;
@@ -332,7 +338,7 @@ __global__ void __launch_bounds__(kSmallThreads) orth_factor_kernel(int m, doubl
     if (threadIdx.x == 0) {
       double b = -1.0;
       int p = j;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+      for (int w = 0; w < nw; ++w)
         if (s_val[w] > b || (s_val[w] == b && s_idx[w] < p)) {
           b = s_val[w];
           p = s_idx[w];
@@ -345,17 +351,27 @@ __global__ void __launch_bounds__(kSmallThreads) orth_factor_kernel(int m, doubl
     if (s_r == j) break;
     const int p = s_idx[0];
     if (p != j) {
-      // swap rows and columns j and p of the full symmetric matrix
-      for (int i = threadIdx.x; i < m; i += blockDim.x) {
-        const double a = W[(size_t)j * ld + i];
-        W[(size_t)j * ld + i] = W[(size_t)p * ld + i];
-        W[(size_t)p * ld + i] = a;
-      }
-      __syncthreads();
-      for (int i = threadIdx.x; i < m; i += blockDim.x) {
-        const double a = W[(size_t)i * ld + j];
-        W[(size_t)i * ld + j] = W[(size_t)i * ld + p];
-        W[(size_t)i * ld + p] = a;
+      // swap rows and columns j < p of the symmetric matrix, on the lower
+      // triangle: each x other than j and p pairs two entries; (p, j) stays
+      for (int x = threadIdx.x; x < m; x += blockDim.x) {
+        if (x == p) continue;
+        double *e1, *e2;
+        if (x == j) {
+          e1 = &W(j, j);
+          e2 = &W(p, p);
+        } else if (x < j) {
+          e1 = &W(j, x);
+          e2 = &W(p, x);
+        } else if (x < p) {
+          e1 = &W(x, j);
+          e2 = &W(p, x);
+        } else {
+          e1 = &W(x, j);
+          e2 = &W(x, p);
+        }
+        const double t = *e1;
+        *e1 = *e2;
+        *e2 = t;
       }
       if (threadIdx.x == 0) {
         const int32_t q = perm[j];
@@ -364,43 +380,59 @@ __global__ void __launch_bounds__(kSmallThreads) orth_factor_kernel(int m, doubl
       }
       __syncthreads();
     }
-    if (threadIdx.x == 0) W[(size_t)j * ld + j] = sqrt(W[(size_t)j * ld + j]);
+    if (threadIdx.x == 0) W(j, j) = sqrt(W(j, j));
     __syncthreads();
-    const double djj = W[(size_t)j * ld + j];
-    for (int i = j + 1 + threadIdx.x; i < m; i += blockDim.x) W[(size_t)i * ld + j] /= djj;
+    const double djj = W(j, j);
+    for (int i = j + 1 + threadIdx.x; i < m; i += blockDim.x) W(i, j) /= djj;
     __syncthreads();
-    // trailing update of the full symmetric trailing block (both triangles,
-    // so that later row / column swaps stay consistent)
-    const int w = m - j - 1;
-    for (int64_t t = threadIdx.x; t < (int64_t)w * w; t += blockDim.x) {
-      const int i = j + 1 + (int)(t / w), l = j + 1 + (int)(t % w);
-      W[(size_t)i * ld + l] -= W[(size_t)i * ld + j] * W[(size_t)l * ld + j];
+    // trailing update of the lower triangle, one warp per row
+    for (int i = j + 1 + warp; i < m; i += nw) {
+      const double wij = W(i, j);
+      for (int l = j + 1 + lane; l <= i; l += 32) W(i, l) -= wij * W(l, j);
     }
     __syncthreads();
   }
   const int r = s_r;
-  // U = L^T (r x r upper); T = Pi U^{-1}: solve U X = I column by column
-  // (X upper), then scatter the rows by the pivots.  X overwrites T's
-  // pivoted rows: T[perm[i], c] = X[i, c].
-  for (int64_t t = threadIdx.x; t < (int64_t)m * m; t += blockDim.x) {
-    const int i = (int)(t / m), c = (int)(t % m);
-    T[(size_t)i * ldt + c] = 0.0;
-  }
-  __syncthreads();
-  // X[i, c] for i <= c < r: back substitution U X = I, U[i][l] = L[l][i] = W[l * ld + i]
-  for (int c = threadIdx.x; c < r; c += blockDim.x) {
-    for (int i = c; i >= 0; --i) {
-      double s = (i == c) ? 1.0 : 0.0;
-      for (int l = i + 1; l <= c; ++l) s -= W[(size_t)l * ld + i] * T[(size_t)perm[l] * ldt + c];
-      T[(size_t)perm[i] * ldt + c] = s / W[(size_t)i * ld + i];
-    }
-  }
-  __syncthreads();
-  for (int64_t t = threadIdx.x; t < (int64_t)m * r; t += blockDim.x) {
-    const int i = (int)(t / r), c = (int)(t % r);
-    T[(size_t)i * ldt + c] *= s_scale[i];
-  }
+  if (packed)
+    for (int i = warp; i < r; i += nw)
+      for (int l = lane; l <= i; l += 32) Wg[(size_t)i * ldg + l] = W(i, l);
+  for (int i = threadIdx.x; i < m; i += blockDim.x) scale[i] = s_scale[i];
   if (threadIdx.x == 0) *rank = r;
+}
+
+// T (m x m, ldt; columns c < r written) = D Pi L^{-T} from orth_factor_kernel:
+// column c solves L^T x = e_c (x[i] = 0 for i > c) by backward substitution,
+// then T[perm[i], c] = x[i] scale[perm[i]].  One warp per column,
+// kSolveWarps columns per block, grid cdiv(m, kSolveWarps); dynamic shared
+// memory as chol_solve_kernel's (k = m).
+__global__ void __launch_bounds__(kSolveWarps * 32) orth_t_kernel(int m, const double *Wg, int ldg,
+                                                                  const double *__restrict__ scale,
+                                                                  const int32_t *__restrict__ perm,
+                                                                  const int32_t *rank, double *T, int ldt, int packed)
+{
+  extern __shared__ double sm[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int r = *rank;
+  if (blockIdx.x * kSolveWarps >= r) return;
+  double *Lp = sm + (size_t)kSolveWarps * m;
+  if (packed) stage_lower(r, Wg, ldg, Lp);
+  const Lower L{packed ? Lp : const_cast<double *>(Wg), ldg, packed};
+  const int c = blockIdx.x * kSolveWarps + warp;
+  if (c >= r) return;
+  double *x = sm + (size_t)warp * m;
+  for (int i = lane; i < m; i += 32) x[i] = i == c ? 1.0 : 0.0;
+  __syncwarp();
+  for (int j = c; j >= 0; --j) {
+    const double xj = x[j] / L(j, j);
+    for (int i = lane; i < j; i += 32) x[i] -= L(j, i) * xj;
+    __syncwarp();
+    if (lane == 0) x[j] = xj;
+  }
+  __syncwarp();
+  for (int i = lane; i < m; i += 32) {
+    const int pi = perm[i];
+    T[(size_t)pi * ldt + c] = x[i] * scale[pi];
+  }
 }
 
 }  // namespace blk

@@ -819,7 +819,7 @@ __global__ void block_fail_kernel(int a, const int32_t *__restrict__ act, PcgSca
 
 // Block PCG on (K^T K) X = B for R columns (schedule MBC_SCHED_BLOCK):
 // O'Leary's block conjugate gradients with the KL preconditioner, search
-// blocks kept orthonormal (rank-revealing Cholesky QR, twice; block.cuh).
+// blocks kept orthonormal (rank-revealing Cholesky QR, one pass; block.cuh).
 // All active columns share one Krylov space, so a column whose own Krylov
 // space converges slowly is helped by the directions the other columns
 // found.  One step, for the active columns (compact, n x a):
@@ -856,14 +856,14 @@ static mbc_status run_block_pcg(Solver &S, int R, PcgWork<double> &w, const LT *
   // matrices (ld R), Gram partials, index lists
   const size_t nv = (size_t)n * R, sm = (size_t)R * R;
   const int chunks = blk::gram_chunks(n);
-  const size_t bytes = sizeof(double) * (6 * nv + 6 * sm + (size_t)chunks * sm + R) + sizeof(int32_t) * (3 * R + 8);
+  const size_t bytes = sizeof(double) * (6 * nv + 6 * sm + (size_t)chunks * sm + 2 * R) + sizeof(int32_t) * (3 * R + 8);
   MBC_TRY(S.blk.reserve(bytes));
   double *base = (double *)S.blk.ptr;
   double *Xa[2] = {base, base + nv}, *Ra[2] = {base + 2 * nv, base + 3 * nv};
   double *P = base + 4 * nv, *V = base + 5 * nv;
   double *G = base + 6 * nv, *Sm = G + sm, *H = Sm + sm, *Wm = H + sm, *T1 = Wm + sm, *T2 = T1 + sm;
-  double *gpart = T2 + sm, *rr = gpart + (size_t)chunks * sm;
-  int32_t *d_act = (int32_t *)(rr + R), *d_loc = d_act + R, *d_perm = d_loc + R, *d_small = d_perm + R;
+  double *gpart = T2 + sm, *rr = gpart + (size_t)chunks * sm, *oscale = rr + R;
+  int32_t *d_act = (int32_t *)(oscale + R), *d_loc = d_act + R, *d_perm = d_loc + R, *d_small = d_perm + R;
   double *Q = w.Tt, *Z = w.Z, *U = w.U, *W = w.W;
   // host view
   std::vector<int32_t> status(R), act, loc;
@@ -887,12 +887,17 @@ static mbc_status run_block_pcg(Solver &S, int R, PcgWork<double> &w, const LT *
                                                                       U, Zm, Rm, w.part, nullptr);
     S.launches += 2;
   };
-  // the small factorizations run in shared memory when their matrix fits
-  const size_t smem_max = sizeof(double) * blk::kSmemDim * blk::kSmemDim;
-  MBC_TRY(allow_max_smem(blk::chol_kernel, smem_max));
-  MBC_TRY(allow_max_smem(blk::chol_solve_kernel, smem_max));
-  MBC_TRY(allow_max_smem(blk::orth_factor_kernel, smem_max));
-  auto smem_of = [](int k) -> size_t { return k <= blk::kSmemDim ? sizeof(double) * k * k : 0; };
+  // the small factorizations keep their matrix's lower triangle in shared
+  // memory (packed) when it fits; the column-parallel solves add one column
+  // per warp
+  auto packed = [](int k) -> int { return k <= blk::kPackedDim; };
+  auto smem_fac = [&](int k) -> size_t { return packed(k) ? sizeof(double) * blk::packed_len(k) : 0; };
+  auto smem_sol = [&](int k) -> size_t { return sizeof(double) * (size_t)blk::kSolveWarps * k + smem_fac(k); };
+  const size_t smem_sol_max = std::max(smem_sol(blk::kPackedDim), smem_sol(blk::kOrthMax));
+  MBC_TRY(allow_max_smem(blk::chol_kernel, smem_fac(blk::kPackedDim)));
+  MBC_TRY(allow_max_smem(blk::orth_factor_kernel, smem_fac(blk::kPackedDim)));
+  MBC_TRY(allow_max_smem(blk::chol_solve_kernel, smem_sol_max));
+  MBC_TRY(allow_max_smem(blk::orth_t_kernel, smem_sol_max));
   // P (n x r, ld r) = an orthonormal basis of the columns of Vin (n x m, ld
   // m; Vin is P's partner buffer V or Z, not needed afterwards), dependent
   // directions dropped; r = 0 when none is left.  One Cholesky QR pass: the
@@ -901,12 +906,14 @@ static mbc_status run_block_pcg(Solver &S, int R, PcgWork<double> &w, const LT *
   // which is all the recursion needs (it never assumes P^T P = I).
   auto orth = [&](const double *Vin, int m, int *r_out) -> mbc_status {
     gram(Vin, m, m, Vin, m, m, Wm);
-    blk::orth_factor_kernel<<<1, blk::kSmallThreads, smem_of(m), st>>>(m, Wm, R, 1e-6, T1, R, d_perm, d_small,
-                                                                        m <= blk::kSmemDim);
+    blk::orth_factor_kernel<<<1, blk::kSmallThreads, smem_fac(m), st>>>(m, Wm, R, 1e-6, oscale, d_perm, d_small,
+                                                                         packed(m));
+    blk::orth_t_kernel<<<cdiv(m, blk::kSolveWarps), blk::kSolveWarps * 32, smem_sol(m), st>>>(
+        m, Wm, R, oscale, d_perm, d_small, T1, R, packed(m));
     MBC_CK(cudaMemcpyAsync(h_small, d_small, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     MBC_CK(cudaStreamSynchronize(st));
     const int r = h_small[0];
-    ++S.launches;
+    S.launches += 2;
     *r_out = r;
     if (r > 0) update(m, r, Vin, m, T1, nullptr, 0, 1.0, P, r);
     return MBC_OK;
@@ -938,9 +945,9 @@ static mbc_status run_block_pcg(Solver &S, int R, PcgWork<double> &w, const LT *
     gram(P, k, k, Q, k, k, G);
     gram(P, k, k, Ra[cur], a, a, Sm);
     MBC_CK(cudaMemsetAsync(d_flag, 0, sizeof(int32_t), st));
-    blk::chol_kernel<<<1, blk::kSmallThreads, smem_of(k), st>>>(k, G, R, d_flag, k <= blk::kSmemDim);
-    blk::chol_solve_kernel<<<1, blk::kSmallThreads, smem_of(k), st>>>(k, G, R, a, Sm, R, 1.0, d_flag,
-                                                                       k <= blk::kSmemDim);
+    blk::chol_kernel<<<1, blk::kSmallThreads, smem_fac(k), st>>>(k, G, R, d_flag, packed(k));
+    blk::chol_solve_kernel<<<cdiv(a, blk::kSolveWarps), blk::kSolveWarps * 32, smem_sol(k), st>>>(
+        k, G, R, a, Sm, R, 1.0, d_flag, packed(k));
     update(k, a, P, k, Sm, Xa[cur], a, 1.0, Xa[cur], a, d_flag);
     update(k, a, Q, k, Sm, Ra[cur], a, -1.0, Ra[cur], a, d_flag);
     // per-column stop test on |r|^2
@@ -1004,8 +1011,8 @@ static mbc_status run_block_pcg(Solver &S, int R, PcgWork<double> &w, const LT *
     // next search block: P = orth(Z + P beta), beta = -(P^T A P)^-1 Q^T Z
     precond(a, Ra[cur], Z);
     gram(Q, k, k, Z, a, a, H);
-    blk::chol_solve_kernel<<<1, blk::kSmallThreads, smem_of(k), st>>>(k, G, R, a, H, R, -1.0, nullptr,
-                                                                       k <= blk::kSmemDim);
+    blk::chol_solve_kernel<<<cdiv(a, blk::kSolveWarps), blk::kSolveWarps * 32, smem_sol(k), st>>>(
+        k, G, R, a, H, R, -1.0, nullptr, packed(k));
     update(k, a, P, k, H, Z, a, 1.0, V, a);
     S.launches += 1;
     MBC_TRY(orth(V, a, &k));
