@@ -184,10 +184,14 @@ class Solver:
 
     def set_factor_tiles(self, tiles: dict):
         """Factor tile shapes (mbc_solver_set_factor_tiles): {"max_ns": [3],
-        "tile_rows": [4]}."""
+        "tile_rows": [4], "tc_min_ns": int (optional; absent keeps the
+        solver's)}."""
         t = _lib.FactorTiles()
+        check(load().mbc_solver_get_factor_tiles(self._h, C.byref(t)), "mbc_solver_get_factor_tiles")
         t.max_ns[:] = [int(v) for v in tiles["max_ns"]]
         t.tile_rows[:] = [int(v) for v in tiles["tile_rows"]]
+        if "tc_min_ns" in tiles:
+            t.tc_min_ns = int(tiles["tc_min_ns"])
         check(load().mbc_solver_set_factor_tiles(self._h, C.byref(t)), "mbc_solver_set_factor_tiles")
         return self
 
@@ -204,6 +208,12 @@ class Solver:
         check(load().mbc_solver_tune_factor(self._h, int(reps), C.byref(t), C.byref(ms), self._sp()),
               "mbc_solver_tune_factor")
         return t.as_dict(), ms.value
+
+    def tensor_grams(self) -> int:
+        """Supernodes of the last factor whose Gram ran on the tensor cores."""
+        c = C.c_int32(0)
+        check(load().mbc_solver_get_tensor_grams(self._h, C.byref(c)), "get_tensor_grams")
+        return c.value
 
     def pivot_retries(self) -> int:
         c = C.c_int32(0)

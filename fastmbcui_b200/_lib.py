@@ -49,10 +49,10 @@ class SolveOptions(C.Structure):
 
 
 class FactorTiles(C.Structure):
-    _fields_ = [("max_ns", C.c_int32 * 3), ("tile_rows", C.c_int32 * 4)]
+    _fields_ = [("max_ns", C.c_int32 * 3), ("tile_rows", C.c_int32 * 4), ("tc_min_ns", C.c_int32)]
 
     def as_dict(self):
-        return {"max_ns": list(self.max_ns), "tile_rows": list(self.tile_rows)}
+        return {"max_ns": list(self.max_ns), "tile_rows": list(self.tile_rows), "tc_min_ns": int(self.tc_min_ns)}
 
 
 class SolveStats(C.Structure):
@@ -88,6 +88,7 @@ SIGNATURES = {
     "mbc_solver_set_factor_tiles": (C.c_int, [_vp, C.POINTER(FactorTiles)]),
     "mbc_solver_get_factor_tiles": (C.c_int, [_vp, C.POINTER(FactorTiles)]),
     "mbc_solver_tune_factor": (C.c_int, [_vp, _i32, C.POINTER(FactorTiles), C.POINTER(C.c_double), _vp]),
+    "mbc_solver_get_tensor_grams": (C.c_int, [_vp, C.POINTER(C.c_int32)]),
     "mbc_solver_create": (C.c_int, [_vp, C.POINTER(Operator), _i32, _vp, C.POINTER(_vp)]),
     "mbc_solver_destroy": (C.c_int, [_vp]),
     "mbc_solver_factor": (C.c_int, [_vp, _vp]),

@@ -38,6 +38,9 @@ struct FactorArgs {
   // has cancelled most of its digits: the supernode is flagged for the FP64
   // retry (FP32 launches); 0 flags only non-positive pivots.
   double pivot_tol;
+  // 1: Theta_s of every supernode of the launch is already in the global
+  // Theta array (gram_tc_kernel, FP32 launches): step 1 only loads it
+  int32_t gram_ready;
   int32_t smem_cap;  // largest n_s kept in shared memory
   int32_t tile_rows; // panel rows per tile
   int32_t *bad_list, *bad_count;
@@ -98,8 +101,13 @@ __global__ void __launch_bounds__(NT) factor_kernel(FactorArgs a, T *__restrict_
   const T coef = (T)a.coef;
   __syncthreads();
 
-  // 1. Gram assembly, entry chunks of NT*EPT upper-triangle entries
-  for (int e0 = 0; e0 < ne; e0 += NT * EPT) {
+  // 1. Gram assembly, entry chunks of NT*EPT upper-triangle entries (or,
+  // with gram_ready, the tensor-core Gram from the global slice)
+  if (a.gram_ready && in_smem) {
+    const T *src = theta + a.th_ptr[s];
+    for (int e = tid; e < ns * ns; e += NT) A[e] = src[e];
+  }
+  for (int e0 = 0; e0 < (a.gram_ready ? 0 : ne); e0 += NT * EPT) {
     int pe[EPT], qe[EPT];
     T acc[EPT];
 #pragma unroll

@@ -15,6 +15,7 @@
 
 #include "block.cuh"
 #include "factor.cuh"
+#include "factor_tc.cuh"
 #include "forces.cuh"
 #include "matvec.cuh"
 #include "matvec_mesh.cuh"
@@ -289,17 +290,64 @@ mbc_status launch_factor_class(FactorArgs a, T *theta, LT *lval, size_t smem, cu
 
 }  // namespace
 
-// Launch the factor kernels over the given per-class supernode lists.
+// Theta of the listed supernodes (FP32) by the tensor-core Gram kernel
+static mbc_status launch_gram(Solver &S, const std::vector<int32_t> &gram, float *theta, cudaStream_t st)
+{
+  MBC_TRY(upload(S.gram_list, gram, st));
+  ftc::GramArgs g{};
+  g.list = (const int32_t *)S.gram_list.ptr;
+  g.count = (int32_t)gram.size();
+  g.set_ptr = S.d_set_ptr();
+  g.set_ind = S.d_set_ind();
+  g.th_ptr = S.d_th_ptr();
+  g.kind = S.op.kind;
+  g.xr = S.x4();
+  g.nr = S.n4();
+  g.zr = S.z4();
+  g.ys = S.y4();
+  g.M = S.op.M;
+  g.ldm = S.op.ldm;
+  g.Pinv = S.d_Pinv();
+  g.nf = S.nf;
+  g.coef = (float)S.op.coef;
+  g.theta = theta;
+  g.err = (int32_t *)S.m_err.ptr;
+  MBC_TRY(allow_max_smem(ftc::gram_tc_kernel, ftc::smem_bytes()));
+  ftc::gram_tc_kernel<<<(unsigned)gram.size(), ftc::kThreads, ftc::smem_bytes(), st>>>(g);
+  ++S.launches;
+  MBC_CKL();
+  S.gram_tc_count += (int32_t)gram.size();
+  return MBC_OK;
+}
+
+// Launch the factor kernels over the given per-class supernode lists.  In
+// FP32 the supernodes with tiles.tc_min_ns <= n_s <= ftc::kMaxNs take their
+// Gram from the tensor cores first (tc_min_ns = 0: none).
 template <typename T, typename LT>
 static mbc_status run_factor(Solver &S, const std::vector<int32_t> *lists, T *theta, LT *lval,
                              double shift, double pivot_tol, int32_t *d_bad_list,
                              int32_t *d_bad_count, cudaStream_t st)
 {
   const Plan &p = *S.plan;
-  for (int c = 0; c < 4; ++c) {
-    const auto &lst = lists[c];
+  std::vector<int32_t> simt[4], tcl[4], gram;
+  const int tc_min = std::is_same<T, float>::value ? S.tiles.tc_min_ns : 0;
+  for (int c = 0; c < 4; ++c)
+    for (int32_t s : lists[c]) {
+      const int ns = p.set_ptr[s + 1] - p.set_ptr[s];
+      if (tc_min > 0 && ns >= tc_min && ns <= ftc::kMaxNs) {
+        tcl[c].push_back(s);
+        gram.push_back(s);
+      } else {
+        simt[c].push_back(s);
+      }
+    }
+  if constexpr (std::is_same<T, float>::value)
+    if (!gram.empty()) MBC_TRY(launch_gram(S, gram, theta, st));
+  for (int job = 0; job < 8; ++job) {
+    const int c = job & 3, ready = job >> 2;
+    const auto &lst = ready ? tcl[c] : simt[c];
     if (lst.empty()) continue;
-    DevMem &dl = S.class_list[c];
+    DevMem &dl = ready ? S.class_list_tc[c] : S.class_list[c];
     MBC_TRY(upload(dl, lst, st));
     int ns_max = 0;
     for (int32_t s : lst) ns_max = std::max(ns_max, p.set_ptr[s + 1] - p.set_ptr[s]);
@@ -324,6 +372,7 @@ static mbc_status run_factor(Solver &S, const std::vector<int32_t> *lists, T *th
     a.coef = S.op.coef;
     a.shift = shift;
     a.pivot_tol = pivot_tol;
+    a.gram_ready = ready;
     a.bad_list = d_bad_list;
     a.bad_count = d_bad_count;
     const int nt = kClassThreads[c];
@@ -389,12 +438,15 @@ mbc_status Solver::factor(cudaStream_t st)
   for (int32_t s = 0; s < p.n_super; ++s) all[s] = s;
   std::vector<int32_t> lists[4];
   split_classes(p, tiles, all, lists);
+  gram_tc_count = 0;
   if (precision == MBC_F64)
     MBC_TRY((run_factor<double, double>(*this, lists, (double *)theta.ptr, (double *)lval.ptr, 0.0,
                                         0.0, d_bad_list, d_bad_count, st)));
   else
     MBC_TRY((run_factor<float, float>(*this, lists, (float *)theta.ptr, (float *)lval.ptr, 0.0,
                                       kF32PivotTol, d_bad_list, d_bad_count, st)));
+  // a tensor-core Gram that stopped on a bounded wait left its Theta unwritten
+  if (gram_tc_count > 0) MBC_TRY(check_device_error(st));
   // supernodes with a non-positive pivot: redo in FP64, then FP64 with a
   // small diagonal shift
   pivot_retries = 0;
@@ -1697,10 +1749,11 @@ mbc_status mbc::Solver::check_device_error(cudaStream_t st)
   MBC_CK(cudaStreamSynchronize(st));
   if (e) {
     MBC_CK(cudaMemsetAsync(m_err.ptr, 0, sizeof(int32_t), st));
-    if (e == 2) return fail(MBC_CUDA_ERROR, "tensor-core matvec: shared memory window not 1024-byte aligned");
+    if (e == 2) return fail(MBC_CUDA_ERROR, "tensor-core kernel: shared memory window not 1024-byte aligned");
     if (e == 3) return fail(MBC_BAD_ARG, "non-finite kernel value: a source coincides with a collocation point");
-    if (e == 4) return fail(MBC_CUDA_ERROR, "INT8 matvec: an index fell outside its buffer (the access was skipped)");
-    return fail(MBC_TIMEOUT, "a bounded device wait expired in the tensor-core matvec");
+    if (e == 4)
+      return fail(MBC_CUDA_ERROR, "tensor-core kernel: an index or size fell outside its buffer (the access was skipped)");
+    return fail(MBC_TIMEOUT, "a bounded device wait expired in a tensor-core kernel");
   }
   return MBC_OK;
 }
@@ -1730,7 +1783,7 @@ extern "C" mbc_status mbc_solver_factor(mbc_solver *s, mbc_stream stream)
 extern "C" void mbc_factor_default_tiles(mbc_factor_tiles *t)
 {
   if (!t) return;
-  *t = mbc_factor_tiles{{32, 64, 128}, {64, 32, 32, 8}};
+  *t = mbc_factor_tiles{{32, 64, 128}, {64, 32, 32, 8}, 64};
 }
 
 static bool tiles_valid(const mbc_factor_tiles &t)
@@ -1738,14 +1791,14 @@ static bool tiles_valid(const mbc_factor_tiles &t)
   if (t.max_ns[0] < 1 || t.max_ns[0] >= t.max_ns[1] || t.max_ns[1] >= t.max_ns[2] || t.max_ns[2] > 144) return false;
   for (int c = 0; c < 4; ++c)
     if (t.tile_rows[c] < 1 || t.tile_rows[c] > 256) return false;
-  return true;
+  return t.tc_min_ns == 0 || (t.tc_min_ns >= mbc::ftc::kMinNs && t.tc_min_ns <= mbc::ftc::kMaxNs);
 }
 
 extern "C" mbc_status mbc_solver_set_factor_tiles(mbc_solver *s, const mbc_factor_tiles *t)
 {
   if (!s || !t) return fail(MBC_BAD_ARG, "NULL solver or tiles");
-  if (!tiles_valid(*t)) return fail(MBC_BAD_ARG, "factor tiles: need 1 <= max_ns[0] < max_ns[1] < max_ns[2] <= 144 "
-                                                 "and 1 <= tile_rows <= 256");
+  if (!tiles_valid(*t)) return fail(MBC_BAD_ARG, "factor tiles: need 1 <= max_ns[0] < max_ns[1] < max_ns[2] <= 144, "
+                                                 "1 <= tile_rows <= 256 and tc_min_ns 0 or 32 .. 192");
   s->s.tiles = *t;
   return MBC_OK;
 }
@@ -1808,6 +1861,19 @@ extern "C" mbc_status mbc_solver_tune_factor(mbc_solver *s, int32_t reps, mbc_fa
           best = t;
         }
       }
+  // the smallest set whose Gram runs on the tensor cores (FP32 factors)
+  if (S.precision != MBC_F64) {
+    const int mins[6] = {0, 32, 48, 64, 96, 128};
+    for (int m : mins) {
+      mbc_factor_tiles t = best;
+      t.tc_min_ns = m;
+      const double tm = time_of(t);
+      if (tm < tbest) {
+        tbest = tm;
+        best = t;
+      }
+    }
+  }
   // then the panel rows, one class at a time
   const int rows[5] = {8, 16, 32, 64, 128};
   for (int c = 0; c < 4; ++c)
@@ -1826,6 +1892,13 @@ extern "C" mbc_status mbc_solver_tune_factor(mbc_solver *s, int32_t reps, mbc_fa
   if (!std::isfinite(tbest)) return fail(MBC_CUDA_ERROR, "factor tuning: no candidate ran");
   if (best_out) *best_out = best;
   if (ms_best) *ms_best = tbest;
+  return MBC_OK;
+}
+
+extern "C" mbc_status mbc_solver_get_tensor_grams(const mbc_solver *s, int32_t *count)
+{
+  if (!s || !count) return fail(MBC_BAD_ARG, "NULL solver or count");
+  *count = s->s.gram_tc_count;
   return MBC_OK;
 }
 

@@ -35,7 +35,7 @@ struct Solver {
   bool graph = false;  // replay PCG iteration blocks as CUDA graphs
   int32_t matvec_impl = MBC_MATVEC_AUTO;
   int32_t fp64_matvec = MBC_FP64_MATVEC_SIMT;
-  mbc_factor_tiles tiles{{32, 64, 128}, {64, 32, 32, 8}};  // factor class bounds and panel rows
+  mbc_factor_tiles tiles{{32, 64, 128}, {64, 32, 32, 8}, 64};  // factor class bounds, panel rows, tensor Gram
   bool oz_ready = false;  // INT8 digit planes of G built for the current geometry
   mutable bool oz_unprepared = false;  // an INT8 launch found its buffers unsized (not run)
   bool oz_slab = false;   // planes rebuilt per matvec, slab by slab (they do not all fit)
@@ -49,6 +49,8 @@ struct Solver {
   DevMem m_P, m_Pinv, m_sup_ptr, m_sup_ind, m_set_ptr, m_set_ind, m_lptr, m_lind, m_rptr, m_rcol,
       m_rmap, m_th_ptr;
   DevMem class_list[4];
+  DevMem class_list_tc[4], gram_list;  // FP32 factor: supernodes whose Gram ran on the tensor cores
+  int32_t gram_tc_count = 0;           // supernodes of the last factor with the tensor-core Gram
   // operator: rows (original order) and sources (new order) as float4
   DevMem m_x4, m_n4, m_y4;
   DevMem m_z4;  // mesh operator: third vertex of every face (x4, n4 hold the first two)

@@ -153,23 +153,32 @@ mbc_status mbc_solver_get_factor(const mbc_solver *s, double *lval_host, double 
  * collocation rows of the K panel a class stages per pass (class 3, and any
  * class whose shared memory would not fit, use at most that many).  The
  * shapes change the order of the Gram sums (results agree to rounding), not
- * the method.  No counterpart in the reference (one thread per supernode,
- * kl_chol.cu:166-223). */
+ * the method.  In FP32 factors, supernodes with tc_min_ns <= n_s <= 192 form
+ * Theta_s on the tensor cores (tcgen05, 3xTF32 with FP32 chunk sums) before
+ * their class kernel factors it; 0 keeps every Gram on the CUDA cores.  FP64
+ * factors and the FP64 retries always use the CUDA cores.  No counterpart in
+ * the reference (one thread per supernode, kl_chol.cu:166-223). */
 typedef struct {
   int32_t max_ns[3];    /* increasing, 1 .. 144 */
   int32_t tile_rows[4]; /* 1 .. 256 */
+  int32_t tc_min_ns;    /* 0, or 32 .. 192 (default 64) */
 } mbc_factor_tiles;
 
 void mbc_factor_default_tiles(mbc_factor_tiles *tiles);
 mbc_status mbc_solver_set_factor_tiles(mbc_solver *s, const mbc_factor_tiles *tiles);
 mbc_status mbc_solver_get_factor_tiles(const mbc_solver *s, mbc_factor_tiles *tiles);
 /* Autotuner: factor this solver `reps` times with each candidate tile shape
- * (class bounds first, then the panel rows of each class in turn, keeping the
- * best so far), time every factor with CUDA events on `stream`, and leave the
+ * (class bounds first, then, for FP32 factors, the tensor-core threshold
+ * tc_min_ns, then the panel rows of each class in turn, keeping the best so
+ * far), time every factor with CUDA events on `stream`, and leave the
  * fastest shapes set on the solver.  best (optional) receives them and
  * ms_best (optional) the best factor time in ms.  The solver ends factored. */
 mbc_status mbc_solver_tune_factor(mbc_solver *s, int32_t reps, mbc_factor_tiles *best,
                                   double *ms_best, mbc_stream stream);
+
+/* Number of supernodes of the last factor whose Theta_s was formed on the
+ * tensor cores (mbc_factor_tiles.tc_min_ns). */
+mbc_status mbc_solver_get_tensor_grams(const mbc_solver *s, int32_t *count);
 
 /* Number of supernodes refactored in FP64 (FP32 solvers: cancelling or
  * non-positive pivots; FP64 solvers: the diagonal-shift retry). */

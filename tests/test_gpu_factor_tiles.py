@@ -33,10 +33,10 @@ def scene():
 @pytest.mark.parametrize("prec,tol", [(F.MBC_F64, 1e-8), (F.MBC_F32, 1e-3)])
 def test_shapes_give_the_same_factor(scene, prec, tol):
     s = _solver(scene, prec)
-    ref, _ = s.factor().get_factor()
-    for tiles in ({"max_ns": [24, 64, 128], "tile_rows": [16, 16, 16, 16]},
-                  {"max_ns": [48, 96, 144], "tile_rows": [128, 8, 64, 32]},
-                  {"max_ns": [8, 16, 32], "tile_rows": [1, 3, 5, 7]}):
+    ref, _ = s.set_factor_tiles(dict(s.factor_tiles(), tc_min_ns=0)).factor().get_factor()
+    for tiles in ({"max_ns": [24, 64, 128], "tile_rows": [16, 16, 16, 16], "tc_min_ns": 0},
+                  {"max_ns": [48, 96, 144], "tile_rows": [128, 8, 64, 32], "tc_min_ns": 0},
+                  {"max_ns": [8, 16, 32], "tile_rows": [1, 3, 5, 7], "tc_min_ns": 0}):
         got, _ = s.set_factor_tiles(tiles).factor().get_factor()
         assert s.factor_tiles() == tiles
         assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= tol, tiles
@@ -46,7 +46,9 @@ def test_invalid_shapes_are_refused(scene):
     s = _solver(scene, F.MBC_F32)
     for bad in ({"max_ns": [64, 32, 128], "tile_rows": [8, 8, 8, 8]},
                 {"max_ns": [32, 64, 200], "tile_rows": [8, 8, 8, 8]},
-                {"max_ns": [32, 64, 128], "tile_rows": [0, 8, 8, 8]}):
+                {"max_ns": [32, 64, 128], "tile_rows": [0, 8, 8, 8]},
+                {"max_ns": [32, 64, 128], "tile_rows": [8, 8, 8, 8], "tc_min_ns": 16},
+                {"max_ns": [32, 64, 128], "tile_rows": [8, 8, 8, 8], "tc_min_ns": 200}):
         with pytest.raises(F.MbcError):
             s.set_factor_tiles(bad)
 
