@@ -53,6 +53,8 @@ WORKLOADS = {
     "sphere": (lambda seed: _sphere(), "unit icosphere subdivision 4, N=Nf=2562, R=6"),
     "large": (lambda seed: _large(seed), "20 boxes x 5000 points above a 400x250 floor, N=Nf=200000, R=120, "
                                          "rho=4 (the floor is static)"),
+    "boxes3": (lambda seed: _large(seed, n_boxes=3, floor=(120, 80)),
+               "3 boxes x 5000 points above a 120x80 floor, N=Nf=24600, R=18, rho=4 (a small case of 'large')"),
 }
 
 
@@ -87,10 +89,10 @@ def _sphere():
     return S.sphere_scene()
 
 
-def _large(seed):
+def _large(seed, **kw):
     from fastmbcui_b200 import scenes as S
 
-    return S.large_scene(seed=seed)
+    return S.large_scene(seed=seed, **kw)
 
 
 def _scene_for(name, seed):
