@@ -958,7 +958,7 @@ def run_probe(args):
     import fastmbcui_b200 as F
 
     sc = _scene_for(args.workload, 4)
-    R = _ncols(sc)
+    R = args.probe_cols or _ncols(sc)
     dev = torch.device("cuda", 0)
     t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
     plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
@@ -1101,6 +1101,8 @@ def main():
     ap.add_argument("--kernel-probe", action="store_true",
                     help="only run a factor and a few K / K^T launches (ncu captures)")
     ap.add_argument("--probe-reps", type=int, default=3)
+    ap.add_argument("--probe-cols", type=int, default=0,
+                    help="with --kernel-probe: columns of the random block (0: the scene's rigid modes)")
     ap.add_argument("--probe-precision", default="f32", choices=["f32", "f64"],
                     help="with --kernel-probe: the FP32 matvec (tensor or SIMT) or the FP64 SIMT matvec")
     ap.add_argument("--probe-solve", action="store_true",

@@ -209,6 +209,12 @@ class Solver:
               "mbc_solver_tune_factor")
         return t.as_dict(), ms.value
 
+    def set_wait_limit(self, polls: int):
+        """Polls before a tensor-core kernel's wait for a partner gives up
+        (mbc_solver_set_wait_limit; 0: the default).  For failure-path tests."""
+        check(load().mbc_solver_set_wait_limit(self._h, int(polls)), "mbc_solver_set_wait_limit")
+        return self
+
     def tensor_grams(self) -> int:
         """Supernodes of the last factor whose Gram ran on the tensor cores."""
         c = C.c_int32(0)

@@ -87,6 +87,9 @@ struct GramArgs {
   float coef;
   float *theta;                // per supernode: n_s x n_s, reversed, column-major
   int32_t *err;                // 1 a bounded wait expired, 2 shared memory misaligned, 4 a set too large
+  // polls after which a wait for a partner gives up (0: tc::kWaitLimit); the
+  // wait that drains the CTA's own MMAs always uses tc::kWaitLimit
+  uint32_t wait_limit;
 };
 
 __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(GramArgs a)
@@ -122,6 +125,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(GramArgs a)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nks = (a.nf + kK - 1) / kK;
   const int nchunks = (nks + kChunk - 1) / kChunk;
+  const uint32_t WL = a.wait_limit ? a.wait_limit : tc::kWaitLimit;
 
   for (int p = tid; p < ns; p += kThreads) {
     const int c = a.set_ind[sb + p];
@@ -162,7 +166,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(GramArgs a)
     for (int ks = 0; ks < nks; ++ks) {
       const int st = ks % kStages;
       // warp-uniform decision: lane 0's view of the failure flag
-      const bool got = tc::mbar_wait_warp(&aempty[st], ((ks / kStages) & 1) ^ 1);
+      const bool got = tc::mbar_wait_warp(&aempty[st], ((ks / kStages) & 1) ^ 1, 0, WL);
       if (__shfl_sync(0xffffffffu, (!got || *vfail) ? 1 : 0, 0)) {
         if (lane == 0) *s_fail = 1;
         break;
@@ -200,8 +204,8 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(GramArgs a)
       const uint32_t boff = 128 * 128;  // operand row 128: block 1's A and B
       for (int ks = 0; ks < nks; ++ks) {
         const int st = ks % kStages, kc = ks % kChunk;
-        if (*vfail || !tc::mbar_wait_one(&afull[st], (ks / kStages) & 1) ||
-            (kc == 0 && ks > 0 && !tc::mbar_wait_one(chunk_free, ((ks / kChunk) - 1) & 1))) {
+        if (*vfail || !tc::mbar_wait_one(&afull[st], (ks / kStages) & 1, 0, WL) ||
+            (kc == 0 && ks > 0 && !tc::mbar_wait_one(chunk_free, ((ks / kChunk) - 1) & 1, 0, WL))) {
           *s_fail = 1;
           break;
         }
@@ -237,7 +241,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(GramArgs a)
     float *A = a.theta + a.th_ptr[s];
     bool ok = true;
     for (int c = 0; c < nchunks; ++c) {
-      if (warp == kAccWarp0 && lane == 0) s_aflag[c & 1] = tc::mbar_wait_one(chunk_full, c & 1, 64) ? 1 : 0;
+      if (warp == kAccWarp0 && lane == 0) s_aflag[c & 1] = tc::mbar_wait_one(chunk_full, c & 1, 64, WL) ? 1 : 0;
       asm volatile("bar.sync %0, 128;" ::"n"(kBarAcc) : "memory");
       // only the flag the polling lane set before the barrier decides here,
       // so that all four warps take the same branch (a warp that left alone

@@ -102,6 +102,7 @@ static int oz_launch(const Solver &S, int R, const double *vin, double *out, con
   a.part = part;
   a.done = done;
   a.err = (int32_t *)S.m_err.ptr;
+  a.wait_limit = S.wait_limit;
   auto mma = [&](int rt0, int tiles) {
     a.rt0 = rt0;
     const unsigned grid = (unsigned)tiles * (unsigned)groups;

@@ -472,6 +472,9 @@ struct OzArgs {
   const int32_t *done;  // PCG all-stopped flag (may be NULL)
   int32_t *err;         // the largest code raised (atomicMax): 1 a bounded wait expired, 2 shared
                         // memory misaligned, 4 an index outside its buffer (access skipped)
+  // polls after which a wait for a partner gives up (0: kWaitLimit); the
+  // waits that drain the CTA's own copies and MMAs always use kWaitLimit
+  uint32_t wait_limit;
 };
 
 // NPH = np / 2 columns per accumulator warp
@@ -509,6 +512,8 @@ __global__ void __launch_bounds__(kThreads, 1) oz_mma_kernel(OzArgs a)
   const int m0 = rt * kM;
   const int nks = nks_for(a.K);
   const int nchunks = nchunks_for(a.K);
+  // the partner-wait limit, read from the parameter bank at each use
+#define WL (a.wait_limit ? a.wait_limit : kWaitLimit)
 
   if (tid == 0) {
     for (int s = 0; s < kASlots; ++s) {
@@ -546,7 +551,7 @@ __global__ void __launch_bounds__(kThreads, 1) oz_mma_kernel(OzArgs a)
       int b_issued = 0, a_issued = 0;
       for (int ks = 0; ks < nks; ++ks) {
         const int sb = ks % kBSlots;
-        if (*vfail || !tc::mbar_wait_one(&bempty[sb], ((ks / kBSlots) & 1) ^ 1, 32)) {
+        if (*vfail || !tc::mbar_wait_one(&bempty[sb], ((ks / kBSlots) & 1) ^ 1, 32, WL)) {
           *s_fail = 1;
           break;
         }
@@ -568,7 +573,7 @@ __global__ void __launch_bounds__(kThreads, 1) oz_mma_kernel(OzArgs a)
             ok = false;
             break;
           }
-          if (!tc::mbar_wait_one(&aempty[sa], ((t / kASlots) & 1) ^ 1, 32)) {
+          if (!tc::mbar_wait_one(&aempty[sa], ((t / kASlots) & 1) ^ 1, 32, WL)) {
             ok = false;
             break;
           }
@@ -593,8 +598,8 @@ __global__ void __launch_bounds__(kThreads, 1) oz_mma_kernel(OzArgs a)
       for (int ks = 0; ks < nks; ++ks) {
         const int kc = ks % kChunkSteps, sb = ks % kBSlots;
         // the B image, and at a chunk start the previous chunk folded out
-        if (*vfail || !tc::mbar_wait_one(&bfull[sb], (ks / kBSlots) & 1) ||
-            (kc == 0 && ks > 0 && !tc::mbar_wait_one(chunk_free, ((ks / kChunkSteps) - 1) & 1, 32))) {
+        if (*vfail || !tc::mbar_wait_one(&bfull[sb], (ks / kBSlots) & 1, 0, WL) ||
+            (kc == 0 && ks > 0 && !tc::mbar_wait_one(chunk_free, ((ks / kChunkSteps) - 1) & 1, 32, WL))) {
           *s_fail = 1;
           break;
         }
@@ -602,7 +607,7 @@ __global__ void __launch_bounds__(kThreads, 1) oz_mma_kernel(OzArgs a)
         bool ok = true;
         for (int p = 0; p < kDigits; ++p) {
           const int t = ks * kDigits + p, sa = t % kASlots;
-          if (!tc::mbar_wait_one(&afull[sa], (t / kASlots) & 1)) {
+          if (!tc::mbar_wait_one(&afull[sa], (t / kASlots) & 1, 0, WL)) {
             ok = false;
             break;
           }
@@ -647,7 +652,7 @@ __global__ void __launch_bounds__(kThreads, 1) oz_mma_kernel(OzArgs a)
     for (int k = 0; k < NPH; ++k) sum[k] = 0.0;
     bool ok = true;
     for (int c = 0; c < nchunks; ++c) {
-      if (aw == 0 && lane == 0) s_aflag[c & 1] = tc::mbar_wait_one(chunk_full, c & 1, 64) ? 1 : 0;
+      if (aw == 0 && lane == 0) s_aflag[c & 1] = tc::mbar_wait_one(chunk_full, c & 1, 64, WL) ? 1 : 0;
       asm volatile("bar.sync %0, %1;" ::"n"(kBarAcc), "n"(kAccWarps * 32) : "memory");
       if (!s_aflag[c & 1]) {
         ok = false;
@@ -717,6 +722,8 @@ __global__ void __launch_bounds__(kThreads, 1) oz_mma_kernel(OzArgs a)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS) : "memory");
   }
 }
+
+#undef WL
 
 }  // namespace oz
 }  // namespace mbc

@@ -141,13 +141,14 @@ __device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes)
                : "memory");
 }
 
-// bounded wait for the phase with the given parity; false on expiry.  Roles
-// that wait long (sleep_ns > 0) back off between polls so that their polling
-// does not take issue slots from the producer warps.
-__device__ __forceinline__ bool mbar_wait_one(uint64_t *bar, uint32_t parity, uint32_t sleep_ns = 0)
+// bounded wait for the phase with the given parity; false on expiry after
+// `limit` polls.  Roles that wait long (sleep_ns > 0) back off between polls
+// so that their polling does not take issue slots from the producer warps.
+__device__ __forceinline__ bool mbar_wait_one(uint64_t *bar, uint32_t parity, uint32_t sleep_ns = 0,
+                                              uint32_t limit = kWaitLimit)
 {
   const uint32_t a = smem_u32(bar);
-  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+  for (uint32_t it = 0; it < limit; ++it) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -164,10 +165,11 @@ __device__ __forceinline__ bool mbar_wait_one(uint64_t *bar, uint32_t parity, ui
 
 // warp-uniform bounded wait: lane 0 polls, the outcome is broadcast and
 // __syncwarp orders the other lanes after lane 0's acquire
-__device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity, uint32_t sleep_ns = 0)
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity, uint32_t sleep_ns = 0,
+                                               uint32_t limit = kWaitLimit)
 {
   int got = 0;
-  if ((threadIdx.x & 31) == 0) got = mbar_wait_one(bar, parity, sleep_ns) ? 1 : 0;
+  if ((threadIdx.x & 31) == 0) got = mbar_wait_one(bar, parity, sleep_ns, limit) ? 1 : 0;
   got = __shfl_sync(0xffffffffu, got, 0);
   __syncwarp();
   return got != 0;
@@ -296,6 +298,9 @@ struct TcArgs {
   double *part;           // columns: per-CTA partials (gridDim.x x R)
   const int32_t *done;    // PCG all-stopped flag (may be NULL)
   int32_t *err;           // 1: a bounded wait expired; 2: shared memory misaligned
+  // polls after which a wait for a partner gives up (0: kWaitLimit); the
+  // waits that drain the CTA's own copies and MMAs always use kWaitLimit
+  uint32_t wait_limit;
 };
 
 template <int DIR>
@@ -331,6 +336,7 @@ __global__ void __launch_bounds__(kThreads, 1) pk_tc_kernel(TcArgs a)
   const int nks = (K_total + kK - 1) / kK;
   const int nchunks = (nks + kChunk - 1) / kChunk;
   const int tcols = 2 * a.tmem_cols;  // [chunk accumulator | running sum]
+  const uint32_t WL = a.wait_limit ? a.wait_limit : kWaitLimit;
 
   if (tid == 0) {
     for (int s = 0; s < kMaxBStages; ++s) {
@@ -413,8 +419,8 @@ __global__ void __launch_bounds__(kThreads, 1) pk_tc_kernel(TcArgs a)
     // ---------------- scheduler: releases the producers step by step ----------------
     for (int ks = 0; ks < nks; ++ks) {
       if (lane == 0 && !*vfail) {
-        if (!mbar_wait_one(&bfull[ks % nbs], (ks / nbs) & 1) ||
-            !mbar_wait_one(&aempty[ks % kAStages], ((ks / kAStages) & 1) ^ 1))
+        if (!mbar_wait_one(&bfull[ks % nbs], (ks / nbs) & 1, 0, WL) ||
+            !mbar_wait_one(&aempty[ks % kAStages], ((ks / kAStages) & 1) ^ 1, 0, WL))
           *s_fail = 1;
       }
       __syncwarp();
@@ -428,7 +434,7 @@ __global__ void __launch_bounds__(kThreads, 1) pk_tc_kernel(TcArgs a)
       int issued = 0;
       for (int ks = 0; ks < nks; ++ks) {
         const int sb = ks % nbs;
-        if (*vfail || !mbar_wait_one(&bempty[sb], ((ks / nbs) & 1) ^ 1, 32)) {
+        if (*vfail || !mbar_wait_one(&bempty[sb], ((ks / nbs) & 1) ^ 1, 32, WL)) {
           *s_fail = 1;
           break;
         }
@@ -460,8 +466,8 @@ __global__ void __launch_bounds__(kThreads, 1) pk_tc_kernel(TcArgs a)
       if (lane == 0 && !*vfail) {
         // the B stage (normally landed long ago), and at a chunk start the
         // previous chunk folded out of the accumulator
-        if (!mbar_wait_one(&bfull[sb], (ks / nbs) & 1) ||
-            (kc == 0 && ks > 0 && !mbar_wait_one(chunk_free, ((ks / kChunk) - 1) & 1)))
+        if (!mbar_wait_one(&bfull[sb], (ks / nbs) & 1, 0, WL) ||
+            (kc == 0 && ks > 0 && !mbar_wait_one(chunk_free, ((ks / kChunk) - 1) & 1, 0, WL)))
           *s_fail = 1;
       }
       __syncwarp();
@@ -498,7 +504,7 @@ __global__ void __launch_bounds__(kThreads, 1) pk_tc_kernel(TcArgs a)
     const uint32_t lane_off = (uint32_t)(q * 32) << 16;
     bool ok = true;
     for (int c = 0; c < nchunks; ++c) {
-      if (warp == kAccWarp0 && lane == 0) s_aflag[c & 1] = mbar_wait_one(chunk_full, c & 1, 64) ? 1 : 0;
+      if (warp == kAccWarp0 && lane == 0) s_aflag[c & 1] = mbar_wait_one(chunk_full, c & 1, 64, WL) ? 1 : 0;
       asm volatile("bar.sync %0, 128;" ::"n"(kBarAcc) : "memory");
       if (!s_aflag[c & 1]) {
         ok = false;

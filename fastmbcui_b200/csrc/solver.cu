@@ -174,6 +174,7 @@ static int tc_launch(const Solver &S, int R, const float *vin, float *out, const
   a.part = part;
   a.done = done;
   a.err = (int32_t *)S.m_err.ptr;
+  a.wait_limit = S.wait_limit;
   const int nks = (int)cdiv(K, tc::kK);
   const int64_t pack_threads = (int64_t)nks * a.np * (tc::kK / 4);
   tc::pack_b_kernel<<<cdiv(pack_threads, 256), 256, 0, st>>>(vin, K, R, a.np, nks, (uint4 *)S.m_bimg.ptr,
@@ -312,6 +313,7 @@ static mbc_status launch_gram(Solver &S, const std::vector<int32_t> &gram, float
   g.coef = (float)S.op.coef;
   g.theta = theta;
   g.err = (int32_t *)S.m_err.ptr;
+  g.wait_limit = S.wait_limit;
   MBC_TRY(allow_max_smem(ftc::gram_tc_kernel, ftc::smem_bytes()));
   ftc::gram_tc_kernel<<<(unsigned)gram.size(), ftc::kThreads, ftc::smem_bytes(), st>>>(g);
   ++S.launches;
@@ -1892,6 +1894,13 @@ extern "C" mbc_status mbc_solver_tune_factor(mbc_solver *s, int32_t reps, mbc_fa
   if (!std::isfinite(tbest)) return fail(MBC_CUDA_ERROR, "factor tuning: no candidate ran");
   if (best_out) *best_out = best;
   if (ms_best) *ms_best = tbest;
+  return MBC_OK;
+}
+
+extern "C" mbc_status mbc_solver_set_wait_limit(mbc_solver *s, uint32_t polls)
+{
+  if (!s) return fail(MBC_BAD_ARG, "NULL solver");
+  s->s.wait_limit = polls;
   return MBC_OK;
 }
 

@@ -55,6 +55,7 @@ struct Solver {
   DevMem m_x4, m_n4, m_y4;
   DevMem m_z4;  // mesh operator: third vertex of every face (x4, n4 hold the first two)
   DevMem m_err;           // set by a tensor-core kernel (1: a bounded wait expired)
+  uint32_t wait_limit = 0;  // polls before a tensor-core kernel's partner wait gives up (0: the default)
   mutable DevMem m_bimg;  // packed TF32 hi/lo image of the tensor-core B operand
   // FP64-accurate INT8 matvec: digit planes and exponents of G per direction
   // (0: rows, 1: columns), and the per-launch digit image of the vector block

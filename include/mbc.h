@@ -176,6 +176,14 @@ mbc_status mbc_solver_get_factor_tiles(const mbc_solver *s, mbc_factor_tiles *ti
 mbc_status mbc_solver_tune_factor(mbc_solver *s, int32_t reps, mbc_factor_tiles *best,
                                   double *ms_best, mbc_stream stream);
 
+/* Failure-path diagnostics: the number of polls after which a wait of the
+ * tensor-core kernels (INT8 and 3xTF32 matvecs, tensor-core Gram) for a
+ * partner role or a copy gives up (0: the default, 2^22).  On expiry the
+ * kernel stops, waits with the default limit for its own copies and MMAs,
+ * frees its tensor memory and returns; the call reports MBC_TIMEOUT and the
+ * solver stays usable.  For tests: a small limit makes the waits expire. */
+mbc_status mbc_solver_set_wait_limit(mbc_solver *s, uint32_t polls);
+
 /* Number of supernodes of the last factor whose Theta_s was formed on the
  * tensor cores (mbc_factor_tiles.tc_min_ns). */
 mbc_status mbc_solver_get_tensor_grams(const mbc_solver *s, int32_t *count);
