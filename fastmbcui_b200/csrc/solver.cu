@@ -886,9 +886,13 @@ __global__ void block_fail_kernel(int a, const int32_t *__restrict__ act, PcgSca
 // w.X holds x0 and w.Rv the residual b - A x0 (new order, n x R); on exit
 // w.X holds the solutions and w.sc the per-column status, iterations and
 // |r|^2.  FP64 throughout (the matvec per the solver's FP64 choice).
-// columns the block PCG keeps while any column iterates (the INT8 matvec's
-// narrowest column group)
-constexpr int kBlockKeep = 16;
+// columns the block PCG keeps while any column iterates.  Narrow INT8
+// matvecs are bound by the digit-plane stream, so a wider tail block costs
+// little: at N = 64000 one launch takes 3.4 ms at 16 columns and 4.1 ms at
+// 48.  Measured on the 32-ellipsoid trajectory (8 poses, B200): 48 gives 4.6 %
+// fewer column-iterations and 2.5 % shorter steps than 16; 64 and 96 lower
+// the iterations further but lengthen the steps.
+constexpr int kBlockKeep = 48;
 
 template <typename LT>
 static mbc_status run_block_pcg(Solver &S, int R, PcgWork<double> &w, const LT *lval, int maxit, double tol,
@@ -1033,8 +1037,8 @@ static mbc_status run_block_pcg(Solver &S, int R, PcgWork<double> &w, const LT *
     // While any column iterates, the block keeps at least kBlockKeep columns:
     // converged ones stay in (their x keeps improving; their stop state is
     // final) and go on feeding the shared Krylov space with directions, at
-    // no matvec cost, since the INT8 matvec's work does not shrink below 16
-    // columns.  The slowest columns' tail is where this pays.
+    // little matvec cost (above).  The slowest columns' tail is where this
+    // pays.
     if (nact > 0 && nact < std::min(a, kBlockKeep)) {
       std::vector<char> in(a, 0);
       for (int j : keep) in[j] = 1;
