@@ -275,6 +275,21 @@ def run_trajectory(args):
     ms_step = _max_over_ranks(dist, float(np.mean(times)))
     value = world * 1000.0 / ms_step
 
+    # accuracy of the timed path: every column's FP64 true residual
+    # |K^T (f - K x)| / |K^T f| of the last timed step, recomputed after the
+    # timing with the FP64 CUDA-core kernels (the ones the parity tests pin to
+    # the oracle)
+    k_last = args.warmup + len(times) - 1
+    s64 = F.Solver(plans[k_last], x=coords[k_last][0], nx=coords[k_last][1], y=coords[k_last][2],
+                   coef=base.coef, precision=F.MBC_F64)
+    f64 = Fm[k_last].double()
+    nb = torch.linalg.norm(s64.apply_KT(f64), dim=0)
+    rel = torch.linalg.norm(s64.apply_KT(f64 - s64.apply_K(X)), dim=0) / torch.clamp(nb, min=1e-300)
+    verify = {"true_relres_max": _max_over_ranks(dist, float(rel.max())), "tol": 1e-8, "columns": R,
+              "step": k_last, "how": "FP64 CUDA-core K and K^T after the timed steps, on the last timed "
+                                     "step's strengths"}
+    del s64, f64
+
     # end to end through the public API, continuing the trajectory: host
     # coordinates and right-hand side in (pinned), the host plan, the factor
     # and the solve (history kept on the device by the TrajectorySolver, as
@@ -327,6 +342,7 @@ def run_trajectory(args):
                   "true_relres_max": max(s_["true_relres_max"] for s_ in stats),
                   "n_converged": [int(s_["n_converged"]) for s_ in stats],
                   "ms": [round(x, 1) for x in times]},
+        "verify": verify,
         "host_plan_ms": round(t_plan * 1000, 1),
         "roofline": _matvec_roofline(st, base.nf, base.n, R, args.matvec, args.fp64_matvec),
         "clocks": clk.summary(),
