@@ -723,7 +723,8 @@ def run_uneven(args):
     dev = torch.device("cuda", 0)
     scs = S.uneven_batch(args.scenes, first_seed=3)
     t = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
-    plans = F.plan_many([(sc.y, sc.rho, sc.lam, sc.max_super) for sc in scs])
+    # --rho: the KL pattern's radius for every scene (0: the scenes' own, 3)
+    plans = F.plan_many([(sc.y, args.rho or sc.rho, sc.lam, sc.max_super) for sc in scs])
     data = [(t(sc.x), t(sc.nx), t(sc.y), t(sc.rhs())) for sc in scs]
     fp64 = args.solver == "fp64"
     rec64 = args.solver in ("fp64", "mixed64")  # FP64 recursion (block PCG)
@@ -757,7 +758,7 @@ def run_uneven(args):
            "config": {"workload": "uneven", "scenes": len(scs), "N": [sc.n for sc in scs],
                       "R": [_ncols(sc) for sc in scs], "timing": "host wall clock around the whole sample",
                       "solver": PRECISION[args.solver], "schedule": SCHEDULE[args.schedule],
-                      "fp64_matvec": args.fp64_matvec},
+                      "fp64_matvec": args.fp64_matvec, "rho": args.rho or scs[0].rho},
            "solve": {"iters_max": [int(r[1]["iters_max"]) for r in res],
                      "n_converged": [int(r[1]["n_converged"]) for r in res],
                      "true_relres_max": max(r[1]["true_relres_max"] for r in res)}}
@@ -1102,6 +1103,10 @@ def main():
     ap.add_argument("--reserve-s", type=float, default=420.0,
                     help="seconds kept for the legs after the timed steps (e2e, plain FP64, ablation, CPU)")
     ap.add_argument("--scenes", type=int, default=8, help="uneven workload: scenes in the sample")
+    ap.add_argument("--rho", type=float, default=5.0,
+                    help="uneven workload: KL pattern radius for every scene (0: the scenes' own, 3; at 3 the "
+                         "densest scenes of the sample do not all reach 1e-8 within 3 x 12000 iterations, at 5 "
+                         "every column does)")
     ap.add_argument("--solver", default="mixed64", choices=["mixed", "flexible", "fp64", "mixed64"],
                     help="trajectory and uneven: residual-replacement mixed PCG, FP64 flexible CG around the "
                          "FP32 PCG (trajectory), or FP64 PCG (pair with --fp64-matvec int8)")
