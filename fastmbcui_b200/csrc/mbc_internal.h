@@ -35,7 +35,7 @@ struct Plan {
 };
 
 // Maximin ordering (maxmin.h:588-665 + preprocess.h:782-831).
-mbc_status build_order(Plan &p);
+mbc_status build_order(Plan &p, int n_threads);
 // MRA pattern (preprocess.h:235-316).
 mbc_status build_pattern(Plan &p, int n_threads);
 // Supernodes and their row sets (preprocess.h:541-671).

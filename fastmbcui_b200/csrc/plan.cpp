@@ -93,7 +93,10 @@ mbc_status fail(mbc_status s, const std::string &msg)
 }
 const char *last_error_cstr() { return g_last_error.c_str(); }
 
-mbc_status build_order(Plan &p)
+// candidate lists at least this long are filtered by several threads
+constexpr int32_t kParallelScan = 4096;
+
+mbc_status build_order(Plan &p, int n_threads)
 {
   const auto t0 = std::chrono::steady_clock::now();
   const int32_t n = p.n;
@@ -129,6 +132,20 @@ mbc_status build_order(Plan &p)
     heap.set(k, std::min(d, 1e16));
   }
   li[1] = n;
+  // The early pivots scan long candidate lists (their parent is the root,
+  // whose list holds every point) of which few pass the distance test: at
+  // N = 64000, 72 % of the 31 M tests fall in lists of 4096 or more and 4 %
+  // pass.  The test depends only on the pivot, so a long list is filtered
+  // by several threads, each keeping its hits in list order, and the hits
+  // are then visited in list order exactly as the serial loop does: the
+  // heap updates, the appended children and the parents are the same.
+#ifdef _OPENMP
+  const int nthr = n_threads > 0 ? n_threads : omp_get_max_threads();
+#else
+  const int nthr = 1;
+  (void)n_threads;
+#endif
+  std::vector<std::vector<std::pair<int32_t, double>>> hits(nthr);
   for (int32_t k = 1; k < n; ++k) {
     const int32_t piv = heap.id[0];
     const double pd = heap.key[0];
@@ -137,19 +154,42 @@ mbc_status build_order(Plan &p)
     const int32_t kmin = li[parent[piv]], kmax = li[parent[piv] + 1];
     li[k + 1] = li[k];
     const double *xp = &x[3 * piv];
-    for (int32_t kk = kmin; kk < kmax; ++kk) {
-      const int32_t j = lj[kk];
-      const double t2 = sq3(xp, &x[3 * j]);
-      if (t2 < pd * pd) {
-        double jd = heap.get(j);
-        if (t2 < jd * jd) {
-          const double nd = std::min(std::sqrt(t2), 1e16);
-          heap.set(j, nd);
-          jd = nd;
+    const double pd2 = pd * pd;
+    auto visit = [&](int32_t j, double t2) {
+      const double t = std::sqrt(t2);  // the same value at both uses below
+      double jd = heap.get(j);
+      if (t2 < jd * jd) {
+        const double nd = std::min(t, 1e16);
+        heap.set(j, nd);
+        jd = nd;
+      }
+      lj.push_back(j);
+      ++li[k + 1];
+      if (t + jd < pd) parent[j] = k;
+    };
+    if (nthr > 1 && kmax - kmin >= kParallelScan) {
+      for (auto &h : hits) h.clear();
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nthr)
+      {
+        const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        const int64_t len = kmax - kmin;
+        const int32_t b = kmin + (int32_t)(len * t / nt), e = kmin + (int32_t)(len * (t + 1) / nt);
+        auto &h = hits[t];
+        for (int32_t kk = b; kk < e; ++kk) {
+          const int32_t j = lj[kk];
+          const double t2 = sq3(xp, &x[3 * j]);
+          if (t2 < pd2) h.emplace_back(j, t2);
         }
-        lj.push_back(j);
-        ++li[k + 1];
-        if (std::sqrt(t2) + jd < pd) parent[j] = k;
+      }
+#endif
+      for (const auto &h : hits)
+        for (const auto &jt : h) visit(jt.first, jt.second);
+    } else {
+      for (int32_t kk = kmin; kk < kmax; ++kk) {
+        const int32_t j = lj[kk];
+        const double t2 = sq3(xp, &x[3 * j]);
+        if (t2 < pd2) visit(j, t2);
       }
     }
   }
@@ -447,7 +487,7 @@ extern "C" mbc_status mbc_plan_create(int32_t n, const double *pts_host,
     p.lambda = o.lambda;
     p.max_super = o.max_super;
     p.pts.assign(pts_host, pts_host + 3 * (size_t)n);
-    mbc_status s = mbc::build_order(p);
+    mbc_status s = mbc::build_order(p, o.n_threads);
     if (s == MBC_OK) s = mbc::build_pattern(p, o.n_threads);
     if (s == MBC_OK) s = mbc::build_supernodes(p);
     if (s != MBC_OK) {

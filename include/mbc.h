@@ -62,7 +62,7 @@ typedef struct {
   double rho;        /* pattern radius factor; used as (double)(float)rho (mfs_torch_ops.cu:114) */
   double lambda;     /* supernode scale ratio, 1.5 in the reference */
   int32_t max_super; /* max columns per supernode, 2048 in the reference */
-  int32_t n_threads; /* host threads for the pattern; 0 = all */
+  int32_t n_threads; /* host threads for the ordering's long scans and the pattern; 0 = all */
 } mbc_plan_options;
 
 typedef struct {
