@@ -81,6 +81,18 @@ class Plan:
               "get_factor_pattern")
         return lp, li[:self.info.factor_nnz]
 
+    def factor_rows(self):
+        """Row-wise view of the factor pattern (the preconditioner's gather
+        order): rptr[n+1], rcol[nnz] (columns, ascending per row), rmap[nnz]
+        (positions in the column-wise lind)."""
+        nnz = max(1, self.info.factor_nnz)
+        rp = np.empty(self.n + 1, np.int32)
+        rc = np.empty(nnz, np.int32)
+        rm = np.empty(nnz, np.int32)
+        check(load().mbc_plan_get_factor_rows(self._h, rp.ctypes.data, rc.ctypes.data, rm.ctypes.data),
+              "get_factor_rows")
+        return rp, rc[:self.info.factor_nnz], rm[:self.info.factor_nnz]
+
 
 def spatial_order(pts) -> np.ndarray:
     """Morton (Z-curve) order of points (n x 3, float32 coordinates):

@@ -90,6 +90,7 @@ SIGNATURES = {
     "mbc_solver_tune_factor": (C.c_int, [_vp, _i32, C.POINTER(FactorTiles), C.POINTER(C.c_double), _vp]),
     "mbc_solver_get_tensor_grams": (C.c_int, [_vp, C.POINTER(C.c_int32)]),
     "mbc_solver_set_wait_limit": (C.c_int, [_vp, C.c_uint32]),
+    "mbc_plan_get_factor_rows": (C.c_int, [_vp, _vp, _vp, _vp]),
     "mbc_solver_create": (C.c_int, [_vp, C.POINTER(Operator), _i32, _vp, C.POINTER(_vp)]),
     "mbc_solver_destroy": (C.c_int, [_vp]),
     "mbc_solver_factor": (C.c_int, [_vp, _vp]),

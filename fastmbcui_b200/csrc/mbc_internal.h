@@ -39,7 +39,7 @@ mbc_status build_order(Plan &p, int n_threads);
 // MRA pattern (preprocess.h:235-316).
 mbc_status build_pattern(Plan &p, int n_threads);
 // Supernodes and their row sets (preprocess.h:541-671).
-mbc_status build_supernodes(Plan &p);
+mbc_status build_supernodes(Plan &p, int n_threads);
 // Morton (Z-curve) order of n points with coordinates at pts[i * stride + 0..2]
 // (mbc_spatial_order).
 mbc_status spatial_order(int32_t n, const float *pts, int32_t stride, int32_t *order);

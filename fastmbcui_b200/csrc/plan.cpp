@@ -342,7 +342,84 @@ mbc_status build_pattern(Plan &p, int n_threads)
   return MBC_OK;
 }
 
-mbc_status build_supernodes(Plan &p)
+namespace {
+
+// Transpose of an n-column CSC pattern (ptr, ind): row i of the result lists
+// its columns in ascending order, with map[t] = the position in ind of that
+// entry (optional), exactly what a serial counting sort over ascending
+// columns gives.  Threads take contiguous column chunks of about equal
+// entries, count their rows, and fill them in column order at offsets that
+// place chunk t's entries of a row after those of chunks 0 .. t-1.
+void transpose_csc(int32_t n, const std::vector<int32_t> &ptr, const std::vector<int32_t> &ind,
+                   std::vector<int32_t> &tptr, std::vector<int32_t> &tind, std::vector<int32_t> *map,
+                   int n_threads)
+{
+  const int64_t nnz = ptr[n];
+  int want = 1;
+#ifdef _OPENMP
+  want = n_threads > 0 ? n_threads : omp_get_max_threads();
+#else
+  (void)n_threads;
+#endif
+  want = (int)std::max<int64_t>(1, std::min<int64_t>(want, nnz / 65536));
+  std::vector<int32_t> c0;   // column chunk bounds, one chunk per thread of the team
+  std::vector<int32_t> cnt;  // per chunk: entries of row i, then its write offset
+  tptr.assign(n + 1, 0);
+  tind.resize(nnz);
+  if (map) map->resize(nnz);
+  int nt = 1;
+#pragma omp parallel num_threads(want)
+  {
+    int t = 0;
+#ifdef _OPENMP
+    t = omp_get_thread_num();
+#endif
+#pragma omp single
+    {
+#ifdef _OPENMP
+      nt = omp_get_num_threads();  // the team actually granted
+#endif
+      c0.assign(nt + 1, n);
+      c0[0] = 0;
+      for (int u = 1; u < nt; ++u)
+        c0[u] = (int32_t)(std::lower_bound(ptr.begin(), ptr.begin() + n + 1, (int32_t)(nnz * u / nt)) -
+                          ptr.begin());
+      cnt.assign((size_t)nt * (n + 1), 0);
+    }
+    int32_t *c = cnt.data() + (size_t)t * (n + 1);
+    for (int32_t j = c0[t]; j < c0[t + 1]; ++j)
+      for (int32_t k = ptr[j]; k < ptr[j + 1]; ++k) ++c[ind[k]];
+#pragma omp barrier
+#pragma omp for schedule(static)
+    for (int32_t i = 0; i < n; ++i) {
+      int32_t tot = 0;
+      for (int u = 0; u < nt; ++u) tot += cnt[(size_t)u * (n + 1) + i];
+      tptr[i + 1] = tot;
+    }
+#pragma omp single
+    for (int32_t i = 0; i < n; ++i) tptr[i + 1] += tptr[i];
+#pragma omp for schedule(static)
+    for (int32_t i = 0; i < n; ++i) {
+      int32_t off = tptr[i];
+      for (int u = 0; u < nt; ++u) {
+        int32_t &e = cnt[(size_t)u * (n + 1) + i];
+        const int32_t m = e;
+        e = off;
+        off += m;
+      }
+    }
+    for (int32_t j = c0[t]; j < c0[t + 1]; ++j)
+      for (int32_t k = ptr[j]; k < ptr[j + 1]; ++k) {
+        const int32_t q = c[ind[k]]++;
+        tind[q] = j;
+        if (map) (*map)[q] = k;
+      }
+  }
+}
+
+}  // namespace
+
+mbc_status build_supernodes(Plan &p, int n_threads)
 {
   const auto t0 = std::chrono::steady_clock::now();
   const int32_t n = p.n;
@@ -374,14 +451,8 @@ mbc_status build_supernodes(Plan &p)
   // super_sparsity (preprocess.h:604-671): the row set of a supernode is the
   // sorted union of its columns' rows.  Walking rows i ascending and the
   // columns J of row i (the transpose) appends i at most once per supernode.
-  std::vector<int32_t> tptr(n + 1, 0), tind(p.ind.size());
-  for (int32_t k = 0; k < (int32_t)p.ind.size(); ++k) ++tptr[p.ind[k] + 1];
-  for (int32_t i = 0; i < n; ++i) tptr[i + 1] += tptr[i];
-  {
-    std::vector<int32_t> fill(tptr.begin(), tptr.end() - 1);
-    for (int32_t j = 0; j < n; ++j)
-      for (int32_t k = p.ptr[j]; k < p.ptr[j + 1]; ++k) tind[fill[p.ind[k]]++] = j;
-  }
+  std::vector<int32_t> tptr, tind;
+  transpose_csc(n, p.ptr, p.ind, tptr, tind, nullptr, n_threads);
   std::vector<int32_t> last(ns, -1), cnt(ns, 0);
   for (int32_t i = 0; i < n; ++i)
     for (int32_t k = tptr[i]; k < tptr[i + 1]; ++k) {
@@ -430,21 +501,9 @@ mbc_status build_supernodes(Plan &p)
     p.th_ptr[s + 1] = p.th_ptr[s] + m * m;
     p.max_set = std::max<int32_t>(p.max_set, (int32_t)m);
   }
-  // row-wise view of L for the gather form of z = L u
-  p.rptr.assign(n + 1, 0);
-  for (int32_t k = 0; k < (int32_t)p.lind.size(); ++k) ++p.rptr[p.lind[k] + 1];
-  for (int32_t i = 0; i < n; ++i) p.rptr[i + 1] += p.rptr[i];
-  p.rcol.resize(p.lind.size());
-  p.rmap.resize(p.lind.size());
-  {
-    std::vector<int32_t> fill(p.rptr.begin(), p.rptr.end() - 1);
-    for (int32_t j = 0; j < n; ++j)
-      for (int32_t k = p.lptr[j]; k < p.lptr[j + 1]; ++k) {
-        const int32_t t = fill[p.lind[k]]++;
-        p.rcol[t] = j;
-        p.rmap[t] = k;
-      }
-  }
+  // row-wise view of L for the gather form of z = L u (columns ascending in
+  // every row: the gather's summation order)
+  transpose_csc(n, p.lptr, p.lind, p.rptr, p.rcol, &p.rmap, n_threads);
   p.t_super_ms = ms_since(t0);
   return MBC_OK;
 }
@@ -489,7 +548,7 @@ extern "C" mbc_status mbc_plan_create(int32_t n, const double *pts_host,
     p.pts.assign(pts_host, pts_host + 3 * (size_t)n);
     mbc_status s = mbc::build_order(p, o.n_threads);
     if (s == MBC_OK) s = mbc::build_pattern(p, o.n_threads);
-    if (s == MBC_OK) s = mbc::build_supernodes(p);
+    if (s == MBC_OK) s = mbc::build_supernodes(p, o.n_threads);
     if (s != MBC_OK) {
       delete pl;
       return s;
@@ -562,5 +621,16 @@ extern "C" mbc_status mbc_plan_get_factor_pattern(const mbc_plan *plan, int32_t 
   const mbc::Plan &p = plan->p;
   if (lptr_host) std::memcpy(lptr_host, p.lptr.data(), sizeof(int32_t) * p.lptr.size());
   if (lind_host) std::memcpy(lind_host, p.lind.data(), sizeof(int32_t) * p.lind.size());
+  return MBC_OK;
+}
+
+extern "C" mbc_status mbc_plan_get_factor_rows(const mbc_plan *plan, int32_t *rptr_host, int32_t *rcol_host,
+                                               int32_t *rmap_host)
+{
+  if (!plan) return fail(MBC_BAD_ARG, "NULL plan");
+  const mbc::Plan &p = plan->p;
+  if (rptr_host) std::memcpy(rptr_host, p.rptr.data(), sizeof(int32_t) * p.rptr.size());
+  if (rcol_host) std::memcpy(rcol_host, p.rcol.data(), sizeof(int32_t) * p.rcol.size());
+  if (rmap_host) std::memcpy(rmap_host, p.rmap.data(), sizeof(int32_t) * p.rmap.size());
   return MBC_OK;
 }

@@ -91,6 +91,11 @@ mbc_status mbc_plan_get_supernodes(const mbc_plan *plan, int32_t *sup_ptr_host,
 /* Supernodal factor pattern, CSC: lptr[n+1], lind[factor_nnz]. */
 mbc_status mbc_plan_get_factor_pattern(const mbc_plan *plan, int32_t *lptr_host,
                                        int32_t *lind_host);
+/* Row-wise view of the factor pattern that the preconditioner's gather
+ * z = L u walks: rptr[n+1]; row i's entries rcol (their columns, ascending)
+ * and rmap (their positions in lind), factor_nnz each.  For parity tests. */
+mbc_status mbc_plan_get_factor_rows(const mbc_plan *plan, int32_t *rptr_host, int32_t *rcol_host,
+                                    int32_t *rmap_host);
 
 /* Morton (Z-curve) order of n points: order_host[k] = index of the k-th point
  * along the curve (21 bits per axis over the points' bounding cube, ties by

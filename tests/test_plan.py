@@ -19,6 +19,16 @@ def assert_same(y, rho=3.0, lam=1.5, max_super=2048):
             assert np.array_equal(g, o[k]), (meth, k)
     assert p.info.n_super == o["n_super"]
     assert p.info.theta_nnz == int(o["th_ptr"][-1])
+    # the row-wise view the preconditioner's gather walks (built by a
+    # parallel transpose): per row, the columns ascending, as a stable
+    # counting sort of lind gives
+    rp, rc, rm = p.factor_rows()
+    lptr, lind = np.asarray(o["lptr"]), np.asarray(o["lind"], np.int64)
+    n = len(lptr) - 1
+    order = np.argsort(lind, kind="stable")
+    assert np.array_equal(rm, order)
+    assert np.array_equal(rc, np.repeat(np.arange(n), np.diff(lptr))[order])
+    assert np.array_equal(rp, np.concatenate([[0], np.cumsum(np.bincount(lind, minlength=n))]))
     return p, o
 
 
