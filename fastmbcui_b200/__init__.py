@@ -336,6 +336,8 @@ def plan_many(specs, threads=None):
     """Host plans of many scenes at once: specs = [(points, rho, lam,
     max_super), ...], planned on a thread pool (the plan code keeps no shared
     state and the binding releases the interpreter lock during the call).
+    The host cores are divided among the pool's plans (each plan's own
+    parallel stages get cores / workers threads), so they do not oversubscribe.
     Returns the Plans in input order, identical to planning them one by one."""
     import os
     from concurrent.futures import ThreadPoolExecutor
@@ -343,9 +345,11 @@ def plan_many(specs, threads=None):
     specs = list(specs)
     if not specs:
         return []
-    workers = threads or min(len(specs), os.cpu_count() or 1)
+    cores = os.cpu_count() or 1
+    workers = threads or min(len(specs), cores)
+    inner = max(1, cores // workers)
     with ThreadPoolExecutor(max_workers=workers) as ex:
-        return list(ex.map(lambda a: Plan(*a), specs))
+        return list(ex.map(lambda a: Plan(*a, n_threads=inner), specs))
 
 
 def solve_many(solvers, Fs, X0s=None, threads=None, factor=True, **opts):
