@@ -81,7 +81,7 @@ def test_mesh_operator_tensor_gram_matches_cuda_cores():
     assert _rel(got, ref) <= 1e-3
 
 
-def test_fp64_factor_keeps_the_cuda_cores(boxes):
+def test_fp64_factor_keeps_the_cuda_cores():
     sc = S.ellipsoids_scene(3, 2000, seed=9)
     plan = F.Plan(sc.y, sc.rho, sc.lam, sc.max_super)
     s = F.Solver(plan, x=_d(sc.x), nx=_d(sc.nx), y=_d(sc.y), coef=sc.coef, precision=F.MBC_F64)
